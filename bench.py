@@ -1,0 +1,338 @@
+"""Benchmark of the TPS warp hot path on B200.
+
+Workload (one "step" = one whole TPS warp job): the large-TPS configuration,
+a 2048 x 2048 x 1024 uint16 blob+fibre volume (8 GiB), 2000 landmark pairs on
+a jittered lattice displaced by 8 random-phase sinusoids (amplitude <= 12) +
+N(0, 1), B-spline control spacing 16, trilinear resampling: FP64 GPU solve,
+FP32 compensated node evaluation, fused B-spline + trilinear resample.
+
+  value   output GVoxel/s with the volume already in HBM (device-timed, CUDA
+          events on the launching stream, max over ranks)
+  e2e     the same job through the operator-level C ABI call with pinned host
+          buffers (H2D of the volume and D2H of the result inside the timing)
+  roofline  the resample kernel: algorithmic bytes (2 x 2 B per voxel + 12 B
+          per node) / its measured duration vs MEASURED_PEAKS.json hbm_gbs
+  cpu_baseline  the FP64 oracle (a restatement of the reference's CPU path)
+          on a bounded slab of the same job, extrapolated, all host threads
+
+The volume (8 GiB) is far larger than L2 (126 MB), so no flush is needed
+between iterations.  `--impl reference` times the reference's CPU path (the
+oracle restatement; the reference itself cannot be built here) on the same
+workload, metric and unit.  With torchrun (N > 1) every rank warps its own
+replica (the path needs no collective); value = all ranks' voxels / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "TPS warp output GVoxel/s + HBM GB/s vs roofline; p50/p99 job latency"
+SHAPE_ZYX = (1024, 2048, 2048)
+N_LANDMARKS = 2000
+G = 16
+SEED = 1237
+WORKLOAD = f"large_tps_{SHAPE_ZYX[2]}x{SHAPE_ZYX[1]}x{SHAPE_ZYX[0]}_u16_n{N_LANDMARKS}_g{G}"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--small", action="store_true", help="256x256x128 case (for profiling captures)")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1].split()[0]))
+                mx = max(mx, float(r[2].split()[0]))
+                for nm, v in zip(names, r[5:9]):
+                    if "Active" in v and "Not" not in v:
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=__import__("torch").device(f"cuda:{local}"))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------- CPU legs
+
+def cpu_reference_rate(vol_zyx_slab, sub, tar, full_planes: int, threads: int = 0):
+    """FP64 oracle on a slab of output planes; extrapolates the job time to the
+    full volume (solve once + per-plane grid and warp).  Returns (GVoxel/s,
+    seconds of CPU work, description)."""
+    from oracle import oracle as O
+    slab = vol_zyx_slab
+    Z, Y, X = slab.shape
+    t0 = time.perf_counter()
+    c, d = O.tps_solve(tar, sub, 0.2, threads)
+    t1 = time.perf_counter()
+    gsz = (O.grid_size(X, G), O.grid_size(Y, G), O.grid_size(Z, G))
+    df = O.tps_grid(tar, c, d, gsz, G, threads=threads)
+    t2 = time.perf_counter()
+    O.tps_warp(slab, df, G, 0, threads)
+    t3 = time.perf_counter()
+    per_plane = ((t2 - t1) + (t3 - t2)) / Z
+    job = (t1 - t0) + per_plane * full_planes
+    vox = X * Y * full_planes
+    desc = (f"FP64 oracle (restatement of the reference CPU path), solve n={len(sub)} in full + grid/warp of a "
+            f"{X}x{Y}x{Z} slab, extrapolated to {full_planes} planes")
+    return vox / job / 1e9, t3 - t0, desc
+
+
+def run_reference(args):
+    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    from terawarp_b200 import synth
+    threads = O.max_threads()
+    slab_planes = 8
+    case = synth.large_tps_case(SEED, "cpu", shape_zyx=(slab_planes, SHAPE_ZYX[1], SHAPE_ZYX[2]), n=N_LANDMARKS,
+                                g=G, n_blobs=2000, n_fibres=200)
+    sub, tar = synth.lattice_landmarks((SHAPE_ZYX[2], SHAPE_ZYX[1], SHAPE_ZYX[0]), N_LANDMARKS, SEED + 7)
+    slab = case.vol.numpy()
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, secs, desc = cpu_reference_rate(slab, sub, tar, SHAPE_ZYX[0], threads)
+        if i >= args.warmup:
+            rates.append(r)
+    v = statistics.median(rates)
+    ms = SHAPE_ZYX[0] * SHAPE_ZYX[1] * SHAPE_ZYX[2] / (v * 1e9) * 1e3
+    line = {"metric": METRIC, "value": v, "unit": "GVoxel/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "volume_xyz": [SHAPE_ZYX[2], SHAPE_ZYX[1], SHAPE_ZYX[0]],
+                       "landmarks": N_LANDMARKS, "grid_spacing": G, "interp": "trilinear"},
+            "cpu_baseline": {"value": v, "unit": "GVoxel/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": "GVoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- our arm
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import terawarp_b200 as tw
+    from terawarp_b200 import synth
+
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    shape = (128, 256, 256) if args.small else SHAPE_ZYX
+    Z, Y, X = shape
+    n = 64 if args.small else N_LANDMARKS
+    case = synth.large_tps_case(SEED + rank, dev, shape_zyx=shape, n=n, g=G)
+    src = case.vol
+    dst = torch.empty_like(src)
+    sub, tar = case.marker_sub, case.marker_tar
+    ctx = tw.Context(local)
+    gsz = (tw.grid_size(X, G), tw.grid_size(Y, G), tw.grid_size(Z, G))
+    nodes = torch.empty((gsz[2], gsz[1], gsz[0], 4), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step(ev=None):
+        t = tw.tps_solve(ctx, tar, sub)                 # FP64 solve (centres = target markers)
+        if ev is not None:
+            ev[0].record()
+        tw.tps_eval_grid(ctx, t, gsz, G, out=nodes, stream=stream)
+        if ev is not None:
+            ev[1].record()
+        tw.warp_tps_device(ctx, nodes, G, src, dst, 0, stream=stream)
+        if ev is not None:
+            ev[2].record()
+        return t
+
+    for _ in range(args.warmup):
+        step().close()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    keep = []
+    barrier(ws)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for i in range(args.steps):
+            evs[i][3].record()
+            keep.append(step(evs[i][:3]))
+        torch.cuda.synchronize()
+        barrier(ws)
+    launches = ctx.kernel_launches - launches0
+    for t in keep:
+        t.close()
+    step_ms = [evs[i][3].elapsed_time(evs[i][2]) for i in range(args.steps)]
+    solve_ms = [evs[i][3].elapsed_time(evs[i][0]) for i in range(args.steps)]
+    eval_ms = [evs[i][0].elapsed_time(evs[i][1]) for i in range(args.steps)]
+    warp_ms = [evs[i][1].elapsed_time(evs[i][2]) for i in range(args.steps)]
+    total_ms = max_over_ranks(sum(step_ms), ws)
+    vox = X * Y * Z
+    value = ws * vox * args.steps / (total_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    alg_bytes = vox * 2 * 2 + 12 * gsz[0] * gsz[1] * gsz[2]
+    warp_avg = statistics.mean(warp_ms)
+    achieved = alg_bytes / (warp_avg / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get(WORKLOAD if not args.small else "small")
+        except Exception:
+            traffic = None
+    pairs = gsz[0] * gsz[1] * gsz[2] * n
+    eval_avg = statistics.mean(eval_ms)
+    clocks = clk.summary()
+    fp32_peak_tflops = 148 * 128 * 2 * (clocks["sm_mhz"] or 1965.0) * 1e6 / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "GVoxel/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16",
+        "data": "synthetic: seeded blob+fibre uint16 volume, jittered-lattice landmarks with sinusoidal displacement",
+        "config": {"workload": WORKLOAD if not args.small else "small_tps_256x256x128_u16_n64_g16",
+                   "volume_xyz": [X, Y, Z], "landmarks": n, "grid_spacing": G, "interp": "trilinear",
+                   "parallelism": f"replicas x{ws}", "l2": "input 8 GiB > 126 MB L2 (no flush needed)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": "k_resample_tps<uint16,16>",
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": warp_avg},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "stages_ms": {"solve_fp64": statistics.mean(solve_ms), "node_eval_fp32": eval_avg, "resample": warp_avg},
+        "tps_eval": {"pairs": pairs, "flop_per_pair": 15, "tflops": pairs * 15 / (eval_avg / 1e3) / 1e12,
+                     "fp32_peak_tflops_at_clock": fp32_peak_tflops,
+                     "frac": pairs * 15 / (eval_avg / 1e3) / 1e12 / fp32_peak_tflops},
+    }
+    # e2e: operator-level call with pinned host buffers
+    if not args.no_e2e:
+        h_src = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+        h_src.copy_(src)
+        h_dst = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+        torch.cuda.synchronize()
+        tw.imgwarp_smallmemory_image(ctx, sub, tar, G, G, G, 1, 0, h_src, out=h_dst)  # warm
+        times = []
+        for _ in range(max(1, min(args.steps, 3))):
+            barrier(ws)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tw.imgwarp_smallmemory_image(ctx, sub, tar, G, G, G, 1, 0, h_src, out=h_dst)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(statistics.mean(times), ws)
+        line["e2e"] = {"value": ws * vox / e2e_s / 1e9, "unit": "GVoxel/s", "h2d_bytes_per_step": vox * 2,
+                       "d2h_bytes_per_step": vox * 2, "path": "tw_imgwarp_smallmemory_image, pinned host buffers",
+                       "ms_per_step": e2e_s * 1e3}
+        equal = bool(torch.equal(h_dst, dst.cpu()))
+        line["e2e"]["matches_device_path"] = equal
+        del h_src, h_dst
+    if rank == 0 and ws == 1 and not args.no_cpu and not args.small:
+        from oracle import oracle as O
+        slab_planes = 8
+        slab = src[:slab_planes].cpu().numpy()
+        r, secs, desc = cpu_reference_rate(slab, sub, tar, Z, 0)
+        line["cpu_baseline"] = {"value": r, "unit": "GVoxel/s", "cores": O.max_threads(), "kind": "port",
+                                "sample": desc, "seconds": secs}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

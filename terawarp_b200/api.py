@@ -1,0 +1,309 @@
+"""Python mirror of the TeraWarp warp operators over the C ABI.
+
+Names, argument order and meaning follow the reference's operator functions
+(q_imgwarp_tps_quicksmallmemory.h:70-74, q_warp_affine_tps.h:66-74) and the
+plugin's parameter surface (plugin_Bigimagewarp.cpp:123-336, README.md:85-100);
+volumes are arrays instead of files.  Every call goes through
+libterawarp_b200.so; nothing here computes a warp in Python.
+
+Volumes are numpy arrays or torch tensors (host, pinned host or CUDA), C
+contiguous, shaped (z, y, x) or (c, z, y, x), dtype uint8 or uint16 -- the
+reference's x-fastest layout (basic_memory.cpp:148-168).  Landmarks are (n, 3)
+arrays of x, y, z voxel coordinates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+
+class TeraWarpError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+def _check(status: int, ctx: Optional["Context"] = None, what: str = "") -> None:
+    if status == L.TW_OK:
+        return
+    lib = L.load()
+    detail = ""
+    if ctx is not None and ctx.handle:
+        detail = (lib.tw_ctx_last_error(ctx.handle) or b"").decode()
+    base = (lib.tw_status_string(status) or b"").decode()
+    raise TeraWarpError(status, f"{what}: {base}" + (f": {detail}" if detail else ""))
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x) -> int:
+    if _is_torch(x):
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        if not x.flags.c_contiguous:
+            raise ValueError("array must be C contiguous")
+        return x.ctypes.data
+    raise TypeError(f"unsupported buffer type {type(x)}")
+
+
+def _dtype_code(x) -> int:
+    if _is_torch(x):
+        import torch
+        if x.dtype == torch.uint8:
+            return L.TW_U8
+        if x.dtype == torch.uint16:
+            return L.TW_U16
+        raise TypeError(f"unsupported dtype {x.dtype}")
+    if x.dtype == np.uint8:
+        return L.TW_U8
+    if x.dtype == np.uint16:
+        return L.TW_U16
+    raise TypeError(f"unsupported dtype {x.dtype}")
+
+
+def _sz4(x) -> "C.Array":
+    shp = tuple(x.shape)
+    if len(shp) == 3:
+        z, y, xx = shp
+        c = 1
+    elif len(shp) == 4:
+        c, z, y, xx = shp
+    else:
+        raise ValueError("volume must be (z, y, x) or (c, z, y, x)")
+    return (C.c_int64 * 4)(xx, y, z, c)
+
+
+def _sz3(x) -> "C.Array":
+    s = _sz4(x)
+    return (C.c_int64 * 3)(s[0], s[1], s[2])
+
+
+def _markers(pts) -> "C.Array":
+    a = np.ascontiguousarray(np.asarray(pts, dtype=np.float32).reshape(-1, 3))
+    arr = (L.tw_marker * max(len(a), 1))()
+    for i, (x, y, z) in enumerate(a):
+        arr[i].x, arr[i].y, arr[i].z = float(x), float(y), float(z)
+    return arr
+
+
+def _like(x, shape):
+    if _is_torch(x):
+        import torch
+        kw = {"dtype": x.dtype, "device": x.device}
+        if x.device.type == "cpu" and x.is_pinned():
+            return torch.empty(shape, pin_memory=True, dtype=x.dtype)
+        return torch.empty(shape, **kw)
+    return np.empty(shape, dtype=x.dtype)
+
+
+class Context:
+    """A device context (tw_ctx): streams, HBM budget, error text."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = L.load()
+        h = C.c_void_p()
+        _check(self.lib.tw_ctx_create(device, hbm_budget_bytes, C.byref(h)), None, "tw_ctx_create")
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.tw_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.tw_ctx_kernel_launches(self.handle))
+
+    def synchronize(self) -> None:
+        _check(self.lib.tw_ctx_synchronize(self.handle), self, "tw_ctx_synchronize")
+
+
+class TPS:
+    """Solved TPS coefficients, device-resident (tw_tps)."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, n: int):
+        self.ctx, self.handle, self.n = ctx, handle, n
+
+    def coeffs(self):
+        c = np.zeros((self.n, 4), np.float64)
+        d = np.zeros((4, 4), np.float64)
+        _check(self.ctx.lib.tw_tps_get_coeffs(self.handle, c.ctypes.data_as(L._DP), d.ctypes.data_as(L._DP)),
+               self.ctx, "tw_tps_get_coeffs")
+        return c, d
+
+    def close(self) -> None:
+        if self.handle:
+            self.ctx.lib.tw_tps_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tps_solve(ctx: Context, centres, values, lam: float = 0.2) -> TPS:
+    """FP64 GPU solve; centres = TPS kernel centres, values = mapped points."""
+    c = _markers(centres)
+    v = _markers(values)
+    n = len(np.asarray(centres).reshape(-1, 3))
+    h = C.c_void_p()
+    _check(ctx.lib.tw_tps_solve(ctx.handle, c, v, n, lam, C.byref(h)), ctx, "tw_tps_solve")
+    return TPS(ctx, h, n)
+
+
+def grid_size(sz: int, g: int) -> int:
+    return int(L.load().tw_grid_size(sz, g))
+
+
+def tps_eval_grid(ctx: Context, tps: TPS, gsz: Sequence[int], g: int, offset=(0, 0, 0), out=None, stream=None):
+    """Node displacements (gz, gy, gx, 4) float32 on the context's device."""
+    import torch
+    gx, gy, gz = (int(v) for v in gsz)
+    if out is None:
+        out = torch.empty((gz, gy, gx, 4), dtype=torch.float32, device=f"cuda:{ctx.device}")
+    _check(ctx.lib.tw_tps_eval_grid(ctx.handle, tps.handle, gx, gy, gz, g, int(offset[0]), int(offset[1]),
+                                    int(offset[2]), C.c_void_p(_ptr(out)), C.c_void_p(stream or 0)),
+           ctx, "tw_tps_eval_grid")
+    return out
+
+
+def warp_tps_device(ctx: Context, nodes, g: int, src, dst, interp: int = 0, stream=None) -> None:
+    """Fused B-spline + resample of device volumes (z, y, x)."""
+    _check(ctx.lib.tw_warp_tps_device(ctx.handle, C.c_void_p(_ptr(nodes)), g, _dtype_code(src), interp,
+                                      C.c_void_p(_ptr(src)), C.c_void_p(_ptr(dst)), _sz3(src),
+                                      C.c_void_p(stream or 0)), ctx, "tw_warp_tps_device")
+
+
+def fit_affine(ctx: Context, tar, sub) -> np.ndarray:
+    """4x4 matrix T with sub = T tar (3-D DLT, FP64 on the GPU)."""
+    M = np.zeros(16, np.float64)
+    n = len(np.asarray(tar).reshape(-1, 3))
+    _check(ctx.lib.tw_fit_affine(ctx.handle, _markers(tar), _markers(sub), n, M.ctypes.data_as(L._DP)), ctx,
+           "tw_fit_affine")
+    return M.reshape(4, 4)
+
+
+def make_affine(warp_mode: int, deformation_mode: int, para, in_sz, out_sz=None) -> np.ndarray:
+    """Pull-back matrix of the scaling / rotation / translation parameters."""
+    out_sz = in_sz if out_sz is None else out_sz
+    M = np.zeros(16, np.float64)
+    p = (C.c_double * 3)(*[float(v) for v in para])
+    a = (C.c_int64 * 3)(*[int(v) for v in in_sz])
+    b = (C.c_int64 * 3)(*[int(v) for v in out_sz])
+    _check(L.load().tw_make_affine(warp_mode, deformation_mode, p, a, b, M.ctypes.data_as(L._DP)), None,
+           "tw_make_affine")
+    return M.reshape(4, 4)
+
+
+def warp_affine_device(ctx: Context, M, src, dst, interp: int = 0, stream=None) -> None:
+    Mx = np.ascontiguousarray(np.asarray(M, np.float64).reshape(16))
+    _check(ctx.lib.tw_warp_affine_device(ctx.handle, Mx.ctypes.data_as(L._DP), _dtype_code(src), interp,
+                                         C.c_void_p(_ptr(src)), _sz3(src), C.c_void_p(_ptr(dst)), _sz3(dst),
+                                         C.c_void_p(stream or 0)), ctx, "tw_warp_affine_device")
+
+
+def imgwarp_smallmemory_image(ctx: Context, ql_marker_tar, ql_marker_sub, szBlock_x: int, szBlock_y: int,
+                              szBlock_z: int, i_interpmethod_df: int, i_interpmethod_img: int, p_img_sub, out=None):
+    """Mirror of imgwarp_smallmemory_image: ql_marker_tar are the TPS values,
+    ql_marker_sub the TPS centres (as the reference function uses them)."""
+    if out is None:
+        out = _like(p_img_sub, tuple(p_img_sub.shape))
+    n = len(np.asarray(ql_marker_tar).reshape(-1, 3))
+    if len(np.asarray(ql_marker_sub).reshape(-1, 3)) != n:
+        raise TeraWarpError(L.TW_ERR_ARG, "target or subject control points is invalid")
+    _check(ctx.lib.tw_imgwarp_smallmemory_image(ctx.handle, _markers(ql_marker_tar), _markers(ql_marker_sub), n,
+                                                szBlock_x, szBlock_y, szBlock_z, i_interpmethod_df,
+                                                i_interpmethod_img, _dtype_code(p_img_sub),
+                                                C.c_void_p(_ptr(p_img_sub)), _sz4(p_img_sub),
+                                                C.c_void_p(_ptr(out))), ctx, "imgwarp_smallmemory_image")
+    return out
+
+
+def q_imagewarp_affine_image(ctx: Context, ql_marker_tar, ql_marker_sub, p_img_sub, out=None):
+    """Mirror of q_imagewarp_affine_image: fits sub = T tar and warps."""
+    if out is None:
+        out = _like(p_img_sub, tuple(p_img_sub.shape))
+    n = len(np.asarray(ql_marker_tar).reshape(-1, 3))
+    if len(np.asarray(ql_marker_sub).reshape(-1, 3)) != n:
+        raise TeraWarpError(L.TW_ERR_ARG, "target or subject control points is invalid")
+    _check(ctx.lib.tw_q_imagewarp_affine_image(ctx.handle, _markers(ql_marker_tar), _markers(ql_marker_sub), n,
+                                               _dtype_code(p_img_sub), C.c_void_p(_ptr(p_img_sub)), _sz4(p_img_sub),
+                                               C.c_void_p(_ptr(out))), ctx, "q_imagewarp_affine_image")
+    return out
+
+
+def params(warp_mode=0, device_mode=1, resize_mode=0, deformation_mode=1, para=(1.0, 1.0, 1.0), newsize=(0, 0, 0),
+           grid_spacing=4, marker_scale=1.0, lam=0.2, interp=0) -> L.tw_params:
+    p = L.tw_params()
+    L.load().tw_params_default(C.byref(p))
+    p.warp_mode, p.device_mode, p.resize_mode, p.deformation_mode = warp_mode, device_mode, resize_mode, \
+        deformation_mode
+    p.para_x, p.para_y, p.para_z = (float(v) for v in para)
+    p.newsize_x, p.newsize_y, p.newsize_z = (int(v) for v in newsize)
+    p.grid_spacing, p.marker_scale, p.lambda_, p.interp = grid_spacing, marker_scale, lam, interp
+    return p
+
+
+def output_size(p: L.tw_params, in_sz) -> tuple:
+    a = (C.c_int64 * 3)(*[int(v) for v in in_sz])
+    b = (C.c_int64 * 3)()
+    _check(L.load().tw_output_size(C.byref(p), a, b), None, "tw_output_size")
+    return tuple(int(v) for v in b)
+
+
+def bigimagewarp(ctx: Context, p_img_sub, marker_sub=None, marker_tar=None, out=None, **kw):
+    """Plugin-level warp with the TeraWarp command's parameters (keyword
+    arguments of `params`)."""
+    p = params(**kw)
+    sz4 = _sz4(p_img_sub)
+    osz = output_size(p, (sz4[0], sz4[1], sz4[2]))
+    shape = (osz[2], osz[1], osz[0]) if len(p_img_sub.shape) == 3 else (sz4[3], osz[2], osz[1], osz[0])
+    if out is None:
+        out = _like(p_img_sub, shape)
+    n = 0 if marker_sub is None else len(np.asarray(marker_sub).reshape(-1, 3))
+    ms = _markers(marker_sub if marker_sub is not None else np.zeros((1, 3)))
+    mt = _markers(marker_tar if marker_tar is not None else np.zeros((1, 3)))
+    _check(ctx.lib.tw_bigimagewarp(ctx.handle, C.byref(p), ms, mt, n, _dtype_code(p_img_sub),
+                                   C.c_void_p(_ptr(p_img_sub)), sz4, C.c_void_p(_ptr(out))), ctx, "tw_bigimagewarp")
+    return out
+
+
+def downsample_factor(sz) -> int:
+    a = (C.c_int64 * 3)(*[int(v) for v in sz])
+    return int(L.load().tw_downsample_factor(a))
+
+
+def downsample_image(ctx: Context, img, out=None):
+    sz4 = _sz4(img)
+    f = downsample_factor((sz4[0], sz4[1], sz4[2]))
+    osz = (sz4[0] // f, sz4[1] // f, sz4[2] // f)
+    shape = (osz[2], osz[1], osz[0]) if len(img.shape) == 3 else (sz4[3], osz[2], osz[1], osz[0])
+    if out is None:
+        out = _like(img, shape)
+    o3 = (C.c_int64 * 3)()
+    _check(ctx.lib.tw_downsample_image(ctx.handle, _dtype_code(img), C.c_void_p(_ptr(img)), sz4,
+                                       C.c_void_p(_ptr(out)), o3), ctx, "tw_downsample_image")
+    return out

@@ -1,0 +1,350 @@
+// tw_api.cpp -- host side of the C ABI: context, solve / evaluate / warp entry
+// points, the reference's operator-level functions and the TeraWarp command's
+// parameter surface.
+#include "tw_internal.h"
+#include "tw_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+using namespace tw;
+
+namespace tw {
+
+tw_status fail(const tw_ctx *ctx, tw_status code, const std::string &msg)
+{
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->err_mu);
+        const_cast<tw_ctx *>(ctx)->last_error = msg;
+    }
+    return code;
+}
+
+tw_status dmalloc(tw_ctx *ctx, void **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) return TW_OK;
+    size_t prev = ctx->used.fetch_add(bytes);
+    if (prev + bytes > ctx->budget) {
+        ctx->used.fetch_sub(bytes);
+        return fail(ctx, TW_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget");
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        ctx->used.fetch_sub(bytes);
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(ctx, TW_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return TW_OK;
+}
+
+void dfree(tw_ctx *ctx, void *p, size_t bytes)
+{
+    if (!p) return;
+    cudaFree(p);
+    ctx->used.fetch_sub(bytes);
+}
+
+int64_t grid_size(int64_t sz, int g) { return (int64_t)std::ceil((double)sz / (double)g) + 3; }
+
+bool is_device_ptr(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+bool is_pinned_ptr(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Device-resident TPS field of one job: coefficients + node grid.
+tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *values, int n, double lambda,
+                   double scale, cudaStream_t st, tw_tps **out)
+{
+    *out = nullptr;
+    if (!centres || !values || n < 4) return fail(ctx, TW_ERR_ARG, "TPS needs n >= 4 landmark pairs");
+    std::unique_ptr<tw_tps> t(new tw_tps);
+    t->ctx = ctx;
+    t->n = n;
+    std::vector<double> hc(3 * (size_t)n), hv(3 * (size_t)n);
+    double o[3] = {0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        // landmarks go through float (Coord3D_JBA) before the FP64 solve,
+        // as in the reference (q_imgwarp_tps_quicksmallmemory.cpp:2039-2046)
+        float cx = (float)(scale * centres[i].x), cy = (float)(scale * centres[i].y), cz = (float)(scale * centres[i].z);
+        float vx = (float)(scale * values[i].x), vy = (float)(scale * values[i].y), vz = (float)(scale * values[i].z);
+        hc[3 * i] = cx; hc[3 * i + 1] = cy; hc[3 * i + 2] = cz;
+        hv[3 * i] = vx; hv[3 * i + 1] = vy; hv[3 * i + 2] = vz;
+        o[0] += cx; o[1] += cy; o[2] += cz;
+    }
+    for (int a = 0; a < 3; ++a) o[a] = std::floor(o[a] / n + 0.5);
+    size_t cbytes = sizeof(double) * 4 * (size_t)n;
+    TW_TRY(dmalloc(ctx, (void **)&t->d_c, cbytes));
+    tw_status s = solve_tps_device(ctx, hc.data(), hv.data(), n, lambda, t->d_c, t->h_d, st);
+    if (s != TW_OK) {
+        dfree(ctx, t->d_c, cbytes);
+        t->d_c = nullptr;
+        return s;
+    }
+    // FP32 evaluation arrays: centres relative to o, negated coefficients
+    std::vector<double> hcoef(4 * (size_t)n);
+    TW_CUDA_TRY(cudaMemcpyAsync(hcoef.data(), t->d_c, cbytes, cudaMemcpyDeviceToHost, st));
+    TW_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<float4> c32(n), k32(n);
+    for (int i = 0; i < n; ++i) {
+        c32[i] = make_float4((float)(hc[3 * i] - o[0]), (float)(hc[3 * i + 1] - o[1]), (float)(hc[3 * i + 2] - o[2]), 0.f);
+        k32[i] = make_float4((float)(-hcoef[4 * i + 1]), (float)(-hcoef[4 * i + 2]), (float)(-hcoef[4 * i + 3]), 0.f);
+    }
+    size_t fbytes = sizeof(float4) * (size_t)n;
+    tw_status s2 = dmalloc(ctx, (void **)&t->d_ctr32, fbytes);
+    if (s2 == TW_OK) s2 = dmalloc(ctx, (void **)&t->d_coef32, fbytes);
+    if (s2 != TW_OK) {
+        dfree(ctx, t->d_c, cbytes);
+        dfree(ctx, t->d_ctr32, fbytes);
+        return s2;
+    }
+    TW_CUDA_TRY(cudaMemcpyAsync(t->d_ctr32, c32.data(), fbytes, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaMemcpyAsync(t->d_coef32, k32.data(), fbytes, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int a = 0; a < 3; ++a) t->o32[a] = o[a];
+    t->h_ctr = new double[3 * (size_t)n];
+    std::memcpy(t->h_ctr, hc.data(), sizeof(double) * 3 * n);
+    *out = t.release();
+    return TW_OK;
+}
+
+void destroy_tps(tw_tps *t)
+{
+    if (!t) return;
+    tw_ctx *ctx = t->ctx;
+    dfree(ctx, t->d_c, sizeof(double) * 4 * (size_t)t->n);
+    dfree(ctx, t->d_ctr32, sizeof(float4) * (size_t)t->n);
+    dfree(ctx, t->d_coef32, sizeof(float4) * (size_t)t->n);
+    delete[] t->h_ctr;
+    delete t;
+}
+
+tw_status eval_grid(tw_ctx *ctx, const tw_tps *t, const int64_t gsz[3], int g, const int64_t off[3], float4 *out,
+                    cudaStream_t st)
+{
+    EvalParams p;
+    p.ctr = t->d_ctr32;
+    p.coef = t->d_coef32;
+    p.n = t->n;
+    const double *d = t->h_d;
+    // f_c(p) = d[0][c] + sum_r p_r d[r+1][c];  with p = o + p':
+    // DF_c = (d[0][c] + o.d[1:4][c] - o_c) + sum_r p'_r (d[r+1][c] - delta)
+    for (int c = 0; c < 3; ++c) {
+        double a0 = d[0 * 4 + c + 1];
+        for (int r = 0; r < 3; ++r) a0 += t->o32[r] * d[(r + 1) * 4 + c + 1];
+        a0 -= t->o32[c];
+        p.a0[c] = (float)a0;
+        for (int r = 0; r < 3; ++r) p.alin[r][c] = (float)(d[(r + 1) * 4 + c + 1] - (r == c ? 1.0 : 0.0));
+    }
+    for (int a = 0; a < 3; ++a) {
+        p.gsz[a] = gsz[a];
+        p.node_o[a] = (int64_t)(-g + off[a] - (int64_t)t->o32[a]);
+    }
+    p.g = g;
+    p.out = out;
+    TW_CUDA_TRY(launch_tps_eval(p, st, ctx->sm_count));
+    count_launch(ctx);
+    return TW_OK;
+}
+
+}  // namespace tw
+
+// ===================================================================== ABI
+
+extern "C" {
+
+const char *tw_status_string(tw_status s)
+{
+    switch (s) {
+    case TW_OK: return "ok";
+    case TW_ERR_ARG: return "invalid argument";
+    case TW_ERR_SINGULAR: return "singular or degenerate landmark system";
+    case TW_ERR_OOM: return "out of memory / over HBM budget";
+    case TW_ERR_CUDA: return "CUDA error";
+    case TW_ERR_TIMEOUT: return "timeout";
+    case TW_ERR_IO: return "tile source/sink callback failed";
+    case TW_ERR_UNSUPPORTED: return "unsupported";
+    case TW_ERR_NOT_READY: return "not ready";
+    }
+    return "unknown status";
+}
+
+int tw_abi_version(void) { return TW_ABI_VERSION; }
+
+tw_status tw_ctx_create(int device, size_t hbm_budget_bytes, tw_ctx **out)
+{
+    if (!out) return TW_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return TW_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return TW_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return TW_ERR_CUDA;
+    std::unique_ptr<tw_ctx> c(new tw_ctx);
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return TW_ERR_CUDA;
+    c->sm_count = prop.multiProcessorCount;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return TW_ERR_CUDA;
+    c->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.9 * (double)fr);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return TW_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking) != cudaSuccess) return TW_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking) != cudaSuccess) return TW_ERR_CUDA;
+    *out = c.release();
+    return TW_OK;
+}
+
+tw_status tw_ctx_destroy(tw_ctx *ctx)
+{
+    if (!ctx) return TW_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->h2d) cudaStreamSynchronize(ctx->h2d);
+    if (ctx->d2h) cudaStreamSynchronize(ctx->d2h);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
+    if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+    delete ctx;
+    return TW_OK;
+}
+
+const char *tw_ctx_last_error(const tw_ctx *ctx)
+{
+    if (!ctx) return "";
+    std::lock_guard<std::mutex> lk(ctx->err_mu);
+    return ctx->last_error.c_str();
+}
+
+uint64_t tw_ctx_kernel_launches(const tw_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
+
+tw_status tw_ctx_synchronize(tw_ctx *ctx)
+{
+    if (!ctx) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->h2d));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->d2h));
+    return TW_OK;
+}
+
+int64_t tw_grid_size(int64_t sz, int g) { return g > 0 && sz > 0 ? grid_size(sz, g) : -1; }
+
+tw_status tw_tps_solve(tw_ctx *ctx, const tw_marker *centres, const tw_marker *values, int n, double lambda,
+                       tw_tps **out)
+{
+    if (!ctx || !out) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    return make_tps(ctx, centres, values, n, lambda, 1.0, ctx->stream, out);
+}
+
+tw_status tw_tps_destroy(tw_tps *tps)
+{
+    if (tps) {
+        cudaSetDevice(tps->ctx->device);
+        destroy_tps(tps);
+    }
+    return TW_OK;
+}
+
+int tw_tps_count(const tw_tps *tps) { return tps ? tps->n : 0; }
+
+tw_status tw_tps_get_coeffs(const tw_tps *tps, double *c, double *d)
+{
+    if (!tps) return TW_ERR_ARG;
+    tw_ctx *ctx = tps->ctx;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (c) {
+        TW_CUDA_TRY(cudaMemcpyAsync(c, tps->d_c, sizeof(double) * 4 * (size_t)tps->n, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+        TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    if (d) std::memcpy(d, tps->h_d, sizeof(double) * 16);
+    return TW_OK;
+}
+
+tw_status tw_tps_eval_grid(tw_ctx *ctx, const tw_tps *tps, int64_t gsz0, int64_t gsz1, int64_t gsz2, int g,
+                           int64_t ox, int64_t oy, int64_t oz, void *dev_nodes, void *stream)
+{
+    if (!ctx || !tps || !dev_nodes || g < 1 || gsz0 < 1 || gsz1 < 1 || gsz2 < 1) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const int64_t gsz[3] = {gsz0, gsz1, gsz2}, off[3] = {ox, oy, oz};
+    TW_TRY(eval_grid(ctx, tps, gsz, g, off, static_cast<float4 *>(dev_nodes), st));
+    if (!stream) TW_CUDA_TRY(cudaStreamSynchronize(st));
+    return TW_OK;
+}
+
+tw_status tw_warp_tps_device(tw_ctx *ctx, const void *dev_nodes, int g, int dtype, int interp, const void *dev_src,
+                             void *dev_dst, const int64_t sz[3], void *stream)
+{
+    if (!ctx || !dev_nodes || !dev_src || !dev_dst || !sz) return TW_ERR_ARG;
+    if (!g_supported(g)) return fail(ctx, TW_ERR_UNSUPPORTED, "grid spacing must be 4, 8, 16, 32 or 64");
+    if ((dtype != TW_U8 && dtype != TW_U16) || (interp != 0 && interp != 1)) return TW_ERR_ARG;
+    if (sz[0] < 1 || sz[1] < 1 || sz[2] < 1) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    RJob j = tps_job(dev_src, sz, dev_dst, sz, static_cast<const float4 *>(dev_nodes), g, dtype, interp);
+    TW_TRY(run_jobs(ctx, &j, 1, st));
+    if (!stream) TW_CUDA_TRY(cudaStreamSynchronize(st));
+    return TW_OK;
+}
+
+tw_status tw_warp_affine_device(tw_ctx *ctx, const double M[16], int dtype, int interp, const void *dev_src,
+                                const int64_t src_sz[3], void *dev_dst, const int64_t dst_sz[3], void *stream)
+{
+    if (!ctx || !M || !dev_src || !dev_dst || !src_sz || !dst_sz) return TW_ERR_ARG;
+    if ((dtype != TW_U8 && dtype != TW_U16) || (interp != 0 && interp != 1)) return TW_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (src_sz[a] < 1 || dst_sz[a] < 1) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    RJob j = affine_job(dev_src, src_sz, dev_dst, dst_sz, M, dtype, interp);
+    TW_TRY(run_jobs(ctx, &j, 1, st));
+    if (!stream) TW_CUDA_TRY(cudaStreamSynchronize(st));
+    return TW_OK;
+}
+
+tw_status tw_fit_affine(tw_ctx *ctx, const tw_marker *tar, const tw_marker *sub, int n, double M[16])
+{
+    if (!ctx || !tar || !sub || !M) return TW_ERR_ARG;
+    if (n < 4) return fail(ctx, TW_ERR_ARG, "affine fit needs n >= 4 landmark pairs");
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    std::vector<double> a(3 * (size_t)n), b(3 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        a[3 * i] = tar[i].x; a[3 * i + 1] = tar[i].y; a[3 * i + 2] = tar[i].z;
+        b[3 * i] = sub[i].x; b[3 * i + 1] = sub[i].y; b[3 * i + 2] = sub[i].z;
+    }
+    return fit_affine_device(ctx, a.data(), b.data(), n, M, ctx->stream);
+}
+
+tw_status tw_make_affine(int warp_mode, int deformation_mode, const double para[3], const int64_t in_sz[3],
+                         const int64_t out_sz[3], double M[16])
+{
+    if (!para || !M || !in_sz || !out_sz) return TW_ERR_ARG;
+    return make_param_affine(warp_mode, deformation_mode, para, in_sz, out_sz, M);
+}
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+// tw_internal.h -- shared internals of libterawarp_b200 (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/terawarp_b200.h"
+
+namespace tw {
+
+// ----------------------------------------------------------------- status
+
+struct Error {
+    tw_status code;
+    std::string msg;
+};
+
+#define TW_CUDA_TRY(expr)                                                              \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return ::tw::fail(ctx, TW_ERR_CUDA, std::string(#expr) + ": " +            \
+                                                    cudaGetErrorString(e_));          \
+    } while (0)
+
+#define TW_TRY(expr)                                                                   \
+    do {                                                                               \
+        tw_status s_ = (expr);                                                         \
+        if (s_ != TW_OK) return s_;                                                    \
+    } while (0)
+
+// ------------------------------------------------------------- resample job
+
+// One warp job as the resample kernel sees it.  All coordinates are voxels;
+// "global" means the full subject / output volume of the job.
+struct RJob {
+    const void *src;       // source buffer, first element = global voxel src_o
+    void *dst;             // output buffer, first element = global output voxel out_o
+    const float4 *nodes;   // TPS node grid (DF, float4), node i at (i-1)g; null for affine
+    int64_t src_py, src_pz;   // source buffer pitches (elements)
+    int64_t dst_py, dst_pz;   // output buffer pitches (elements)
+    int64_t src_o[3];      // global coords of the source buffer's first voxel
+    int64_t src_n[3];      // source buffer dims
+    int64_t glob[3];       // subject volume dims (OOB rule q in [0, glob-1])
+    int64_t out_o[3];      // global output coords of this job's region (multiple of g for TPS)
+    int64_t out_n[3];      // region dims
+    int64_t gsz[3];        // node grid dims
+    double M[12];          // affine rows (kind 0)
+    int64_t bricks[3];     // brick counts along x, y, z
+    int64_t brick_begin;   // first flattened brick index of this job in its launch
+    int g;                 // grid spacing (TPS)
+    int dtype;             // 1 u8, 2 u16
+    int kind;              // 0 affine, 1 TPS
+    int interp;            // 0 trilinear, 1 nearest
+};
+
+// Launch one resample pass over `njobs` jobs that share (dtype, kind, g).
+// jobs_dev is device memory holding the RJob array; total_bricks is the sum
+// of all jobs' bricks.  Returns a cudaError_t from the launch.
+cudaError_t launch_resample(const RJob *jobs_dev, int njobs, int64_t total_bricks, int dtype,
+                            int kind, int g, int interp, cudaStream_t st, int sm_count);
+// Brick extents for a (kind, g) pair.
+void brick_dims(int kind, int g, int64_t out[3]);
+
+// ---------------------------------------------------------------- TPS eval
+
+struct EvalParams {
+    const float4 *ctr;     // n centres, relative to the job origin `o`
+    const float4 *coef;    // n coefficients (-c_x, -c_y, -c_z, 0)
+    int n;
+    float a0[3];           // affine part at the origin minus the origin
+    float alin[3][3];      // alin[r][c] = d[r+1][c+1] - delta(r,c)
+    int64_t gsz[3];
+    int g;
+    int64_t node_o[3];     // position of node (0,0,0) relative to the origin
+    float4 *out;
+};
+cudaError_t launch_tps_eval(const EvalParams &p, cudaStream_t st, int sm_count);
+
+// ------------------------------------------------------------------- solve
+
+struct SolveWork;   // device workspace of one solve
+tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
+                           double *d_c_out /*n x 4 device*/, double *h_d_out /*4x4 host*/,
+                           cudaStream_t st);
+tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_sub, int n, double M[16],
+                            cudaStream_t st);
+
+// --------------------------------------------------------------- helpers
+
+int64_t grid_size(int64_t sz, int g);
+bool g_supported(int g);
+
+}  // namespace tw
+
+// ------------------------------------------------------------- the context
+
+struct tw_ctx {
+    int device = 0;
+    int sm_count = 148;
+    size_t budget = 0;
+    std::atomic<size_t> used{0};
+    cudaStream_t stream = nullptr;      // compute
+    cudaStream_t h2d = nullptr;         // host -> device copies
+    cudaStream_t d2h = nullptr;         // device -> host copies
+    std::atomic<uint64_t> launches{0};
+    mutable std::mutex err_mu;
+    std::string last_error;
+};
+
+struct tw_tps {
+    tw_ctx *ctx = nullptr;
+    int n = 0;
+    double *d_c = nullptr;     // device n x 4 (FP64)
+    double h_d[16] = {0};      // host 4 x 4 (FP64)
+    float4 *d_ctr32 = nullptr; // centres, FP32, relative to origin o32
+    float4 *d_coef32 = nullptr;
+    double o32[3] = {0, 0, 0};
+    double *h_ctr = nullptr;   // host copy of centres (FP64 from float input)
+};
+
+namespace tw {
+tw_status fail(const tw_ctx *ctx, tw_status code, const std::string &msg);
+// Budgeted device allocation.
+tw_status dmalloc(tw_ctx *ctx, void **p, size_t bytes);
+void dfree(tw_ctx *ctx, void *p, size_t bytes);
+inline void count_launch(tw_ctx *ctx, uint64_t k = 1) { if (ctx) ctx->launches += k; }
+}  // namespace tw

@@ -1,0 +1,611 @@
+// tw_resample.cu -- fused cubic B-spline expansion + trilinear/NN resampling
+// of uint8/uint16 volumes on sm_100a, for TPS (node-grid) and affine warps.
+//
+// Work unit: a "brick" of output voxels.  One CTA of 256 threads (32 x 8)
+// owns a brick; each thread owns runs of 8 consecutive output voxels along x,
+// so every output row is written with one 16-byte (u16) or 8-byte (u8)
+// vector store per thread, coalesced across the warp.  A launch covers the
+// bricks of one or more jobs that share (dtype, kind, g): the flattened brick
+// index is mapped to its job by a binary search over the jobs' prefix sums,
+// so uneven edge tiles and many small jobs run in one persistent launch.
+//
+// TPS bricks (reference: q_dfblcokinterp_bspline + q_imgblockwarp,
+// q_imgwarp_tps_quicksmallmemory.cpp:85-203, and chazhi.cu:226-338, which
+// does a dense 64x64x3 matvec per 4^3 cell): the cubic B-spline is evaluated
+// separably.  Per brick the 4 x (CY+3) x (CX+3) nodes are staged in shared
+// memory as node' = DF + node position - brick origin (the B-spline
+// reproduces linear functions, so the spline of node' is the sample position
+// q itself, relative to the brick origin).  They are contracted along y once
+// per brick (R), along z once per output slice (Q), and along x per voxel
+// (12 FMA), i.e. ~14 FMA per voxel instead of 192.
+//
+// Sampling follows the reference exactly: a sample with any q_i < 0 or
+// q_i > sz_i - 1 writes 0; weights come from floor(q); TPS rounds with +0.5
+// and truncates, affine truncates (q_warp_affine_tps.cpp:1433).  A brick whose
+// whole sample hull (convex-hull property of the B-spline: weights are >= 0
+// and sum to 1) lies strictly inside the source takes a fast path with no
+// per-voxel bounds tests.
+
+#include "tw_internal.h"
+
+#include <cstdint>
+
+namespace tw {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTX = 32;
+constexpr int kTY = 8;
+constexpr int kV = 8;                 // voxels per thread along x
+constexpr int kBX = kTX * kV;         // 256 voxels per brick along x
+constexpr float kMagic = 12582912.0f; // 1.5 * 2^23: add.rm(q, kMagic) = kMagic + floor(q)
+constexpr int kMagicBits = 0x4B400000;
+
+template <int G>
+struct Geom {
+    static constexpr int BX = kBX;
+    static constexpr int BY = G < 8 ? 8 : G;
+    static constexpr int BZ = G;
+    static constexpr int CX = BX / G;
+    static constexpr int CY = BY / G;
+    static constexpr int NX = CX + 3;
+    static constexpr int NY = CY + 3;
+    static constexpr int NT = 4 + (kV - 1) / G;  // node taps a thread's 8-voxel run touches
+    static constexpr int ROWS = BY / kTY;
+    static constexpr int ND = 4 * NY * NX;       // staged nodes
+    static constexpr int NR = BY * 4 * NX;       // y-contracted
+    static constexpr int NQ = 2 * BY * NX;       // z-contracted, double-buffered
+    static constexpr int UNION = ND > NQ ? ND : NQ;
+    static constexpr size_t smem_bytes = sizeof(float4) * (size_t)(UNION + NR + G) + 64;
+};
+
+// Uniform cubic B-spline blending weights at t = i/g (rows of T*B/6,
+// q_imgwarp_tps_quicksmallmemory.cpp:671-689), evaluated in double and
+// rounded once to float.
+__device__ __forceinline__ float4 bspline_w(int i, int g)
+{
+    double t = (double)i / (double)g;
+    double t2 = t * t, t3 = t2 * t;
+    double w0 = (-t3 + 3.0 * t2 - 3.0 * t + 1.0) / 6.0;
+    double w1 = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
+    double w2 = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
+    double w3 = t3 / 6.0;
+    return make_float4((float)w0, (float)w1, (float)w2, (float)w3);
+}
+
+template <typename T>
+__device__ __forceinline__ float ldv(const T *p)
+{
+    return (float)__ldg(p);
+}
+
+__device__ __forceinline__ float floor_magic(float q, int &i)
+{
+    float m = __fadd_rd(q, kMagic);
+    i = __float_as_int(m) - kMagicBits;
+    return m - kMagic;
+}
+
+// Output conversion: TPS rounds (+0.5) then truncates; affine truncates.
+template <typename T, bool ROUND>
+__device__ __forceinline__ uint32_t to_out(float v)
+{
+    float r = ROUND ? v + 0.5f : v;
+    r = fmaxf(r, 0.0f);
+    uint32_t u = (uint32_t)(__float_as_int(__fadd_rd(r, 8388608.0f)) - 0x4B000000);
+    const uint32_t mx = sizeof(T) == 1 ? 255u : 65535u;
+    return u > mx ? mx : u;
+}
+
+// Trilinear sample at brick-relative position (qx,qy,qz) from `base`
+// (the source element at the brick origin), no bounds tests.
+template <typename T>
+__device__ __forceinline__ float tri_fast(const T *__restrict__ base, int py, int pz, float qx, float qy,
+                                          float qz)
+{
+    int ix, iy, iz;
+    float fx = qx - floor_magic(qx, ix);
+    float fy = qy - floor_magic(qy, iy);
+    float fz = qz - floor_magic(qz, iz);
+    const T *p = base + (iz * pz + iy * py + ix);
+    float v000 = ldv(p), v100 = ldv(p + 1);
+    float v010 = ldv(p + py), v110 = ldv(p + py + 1);
+    float v001 = ldv(p + pz), v101 = ldv(p + pz + 1);
+    float v011 = ldv(p + pz + py), v111 = ldv(p + pz + py + 1);
+    float a0 = fmaf(fx, v100 - v000, v000);
+    float a1 = fmaf(fx, v110 - v010, v010);
+    float a2 = fmaf(fx, v101 - v001, v001);
+    float a3 = fmaf(fx, v111 - v011, v011);
+    float b0 = fmaf(fy, a1 - a0, a0);
+    float b1 = fmaf(fy, a3 - a2, a2);
+    return fmaf(fz, b1 - b0, b0);
+}
+
+// General sample: global position gq (as brick-relative q plus the brick's
+// global origin), reference OOB rule against glob, indices clamped to the
+// source buffer.  Returns false when the reference would write 0.
+template <typename T, int INTERP>
+__device__ __forceinline__ bool sample_slow(const RJob &J, const int64_t O[3], float qx, float qy, float qz,
+                                            float &out)
+{
+    const float q[3] = {qx, qy, qz};
+    int64_t fl[3];
+    float fr[3];
+    for (int a = 0; a < 3; ++a) {
+        // global coordinate check: 0 <= O + q <= glob - 1
+        double gq = (double)O[a] + (double)q[a];
+        if (!(gq >= 0.0) || gq > (double)(J.glob[a] - 1)) return false;
+        double f = floor(gq);
+        fl[a] = (int64_t)f;
+        fr[a] = (float)(gq - f);
+    }
+    const T *src = static_cast<const T *>(J.src);
+    if (INTERP == 1) {
+        int64_t nn[3];
+        for (int a = 0; a < 3; ++a) {
+            double gq = (double)O[a] + (double)q[a];
+            int64_t v = (int64_t)(gq + 0.5);
+            nn[a] = v < J.glob[a] ? v : J.glob[a] - 1;
+            int64_t li = nn[a] - J.src_o[a];
+            li = li < 0 ? 0 : (li >= J.src_n[a] ? J.src_n[a] - 1 : li);
+            nn[a] = li;
+        }
+        out = ldv(src + nn[2] * J.src_pz + nn[1] * J.src_py + nn[0]);
+        return true;
+    }
+    int64_t i0[3], i1[3];
+    for (int a = 0; a < 3; ++a) {
+        int64_t lo = fl[a] - J.src_o[a];
+        int64_t hi = (fl[a] + 1 < J.glob[a] ? fl[a] + 1 : fl[a]) - J.src_o[a];
+        lo = lo < 0 ? 0 : (lo >= J.src_n[a] ? J.src_n[a] - 1 : lo);
+        hi = hi < 0 ? 0 : (hi >= J.src_n[a] ? J.src_n[a] - 1 : hi);
+        i0[a] = lo;
+        i1[a] = hi;
+    }
+    const int64_t r00 = i0[2] * J.src_pz + i0[1] * J.src_py, r10 = i0[2] * J.src_pz + i1[1] * J.src_py;
+    const int64_t r01 = i1[2] * J.src_pz + i0[1] * J.src_py, r11 = i1[2] * J.src_pz + i1[1] * J.src_py;
+    float v000 = ldv(src + r00 + i0[0]), v100 = ldv(src + r00 + i1[0]);
+    float v010 = ldv(src + r10 + i0[0]), v110 = ldv(src + r10 + i1[0]);
+    float v001 = ldv(src + r01 + i0[0]), v101 = ldv(src + r01 + i1[0]);
+    float v011 = ldv(src + r11 + i0[0]), v111 = ldv(src + r11 + i1[0]);
+    float a0 = fmaf(fr[0], v100 - v000, v000);
+    float a1 = fmaf(fr[0], v110 - v010, v010);
+    float a2 = fmaf(fr[0], v101 - v001, v001);
+    float a3 = fmaf(fr[0], v111 - v011, v011);
+    float b0 = fmaf(fr[1], a1 - a0, a0);
+    float b1 = fmaf(fr[1], a3 - a2, a2);
+    out = fmaf(fr[2], b1 - b0, b0);
+    return true;
+}
+
+template <typename T, int INTERP>
+__device__ __forceinline__ float sample_fast(const T *__restrict__ base, int py, int pz, float qx, float qy,
+                                             float qz)
+{
+    if (INTERP == 1) {
+        int ix, iy, iz;
+        floor_magic(qx + 0.5f, ix);
+        floor_magic(qy + 0.5f, iy);
+        floor_magic(qz + 0.5f, iz);
+        return ldv(base + (iz * pz + iy * py + ix));
+    }
+    return tri_fast<T>(base, py, pz, qx, qy, qz);
+}
+
+// Writes a thread's run of 8 voxels.
+template <typename T>
+__device__ __forceinline__ void store_run(T *dst, const uint32_t (&v)[kV], bool vec, int nvalid)
+{
+    if (vec) {
+        if (sizeof(T) == 2) {
+            uint4 w;
+            w.x = v[0] | (v[1] << 16);
+            w.y = v[2] | (v[3] << 16);
+            w.z = v[4] | (v[5] << 16);
+            w.w = v[6] | (v[7] << 16);
+            *reinterpret_cast<uint4 *>(dst) = w;
+        } else {
+            uint2 w;
+            w.x = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
+            w.y = v[4] | (v[5] << 8) | (v[6] << 16) | (v[7] << 24);
+            *reinterpret_cast<uint2 *>(dst) = w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kV; ++i)
+            if (i < nvalid) dst[i] = (T)v[i];
+    }
+}
+
+__device__ __forceinline__ int find_job(const RJob *jobs, int njobs, int64_t b)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].brick_begin <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Block-wide min/max reduction of 3 components (6 floats), result broadcast.
+__device__ __forceinline__ void block_minmax(float (&mn)[3], float (&mx)[3], float *red)
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+        }
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            red[warp * 6 + a] = mn[a];
+            red[warp * 6 + 3 + a] = mx[a];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float m0 = red[a], m1 = red[3 + a];
+        for (int w = 1; w < kThreads / 32; ++w) {
+            m0 = fminf(m0, red[w * 6 + a]);
+            m1 = fmaxf(m1, red[w * 6 + 3 + a]);
+        }
+        mn[a] = m0;
+        mx[a] = m1;
+    }
+}
+
+// Is every brick-relative sample position in [lo, hi] strictly inside both
+// the subject volume and the source buffer, and are all byte offsets
+// representable in 32 bits?
+__device__ __forceinline__ bool hull_inside(const RJob &J, const int64_t O[3], const float (&lo)[3],
+                                            const float (&hi)[3])
+{
+    const float margin = 1.0f / 64.0f;
+    int64_t span = 0;
+    const int64_t pitch[3] = {1, J.src_py, J.src_pz};
+    for (int a = 0; a < 3; ++a) {
+        // subject volume: 0 <= O + q and O + q < glob - 1 (so floor+1 is in range)
+        double glo = (double)O[a] + (double)lo[a] - margin;
+        double ghi = (double)O[a] + (double)hi[a] + margin;
+        if (!(glo >= 0.0) || !(ghi < (double)(J.glob[a] - 1))) return false;
+        // source buffer covers [src_o, src_o + src_n - 1]
+        if (!(glo >= (double)J.src_o[a]) || !(ghi < (double)(J.src_o[a] + J.src_n[a] - 1))) return false;
+        double ext = fmax(fabs((double)lo[a]), fabs((double)hi[a])) + 2.0;
+        span += (int64_t)ext * pitch[a];
+    }
+    return span < (int64_t)0x7fffffff / 2;
+}
+
+// ------------------------------------------------------------------ TPS
+
+template <typename T, int G, int INTERP>
+__device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, float4 *sm, float *red)
+{
+    using Gm = Geom<G>;
+    float4 *Nd = sm;                       // [4][NY][NX]   (aliases Q)
+    float4 *Qb = sm;                       // [2][BY][NX]
+    float4 *R = sm + Gm::UNION;            // [BY][4][NX]
+    const float4 *W = sm + Gm::UNION + Gm::NR;  // [G] weights
+    const int tid = threadIdx.x;
+    const int tx = tid & 31, ty = tid >> 5;
+
+    const int64_t O[3] = {J.out_o[0] + bx * Gm::BX, J.out_o[1] + by * Gm::BY, J.out_o[2] + bz * Gm::BZ};
+    const int64_t c0[3] = {O[0] / G, O[1] / G, O[2] / G};  // first cell (= first node index)
+
+    // 1. stage node' = DF + node position - O, and its hull
+    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    for (int i = tid; i < Gm::ND; i += kThreads) {
+        int nx = i % Gm::NX, t = i / Gm::NX;
+        int ny = t % Gm::NY, nz = t / Gm::NY;
+        int64_t gx = c0[0] + nx, gy = c0[1] + ny, gz = c0[2] + nz;
+        gx = gx < J.gsz[0] ? gx : J.gsz[0] - 1;
+        gy = gy < J.gsz[1] ? gy : J.gsz[1] - 1;
+        gz = gz < J.gsz[2] ? gz : J.gsz[2] - 1;
+        float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
+        // node gx sits at (gx-1)*G; relative to O that is (gx-1)*G - O (exact in float)
+        float4 v;
+        v.x = d.x + (float)((gx - 1) * G - O[0]);
+        v.y = d.y + (float)((gy - 1) * G - O[1]);
+        v.z = d.z + (float)((gz - 1) * G - O[2]);
+        v.w = 0.f;
+        Nd[i] = v;
+        mn[0] = fminf(mn[0], v.x); mn[1] = fminf(mn[1], v.y); mn[2] = fminf(mn[2], v.z);
+        mx[0] = fmaxf(mx[0], v.x); mx[1] = fmaxf(mx[1], v.y); mx[2] = fmaxf(mx[2], v.z);
+    }
+    block_minmax(mn, mx, red);  // contains __syncthreads (Nd visible after it)
+
+    const bool inside_out = (O[0] + Gm::BX <= J.out_o[0] + J.out_n[0]) &&
+                            (O[1] + Gm::BY <= J.out_o[1] + J.out_n[1]) &&
+                            (O[2] + Gm::BZ <= J.out_o[2] + J.out_n[2]);
+    const bool fast = inside_out && hull_inside(J, O, mn, mx);
+
+    // 2. R[y][c][nx] = sum_b wy_b(y) Nd[c][y/G + b][nx]
+    for (int i = tid; i < Gm::NR; i += kThreads) {
+        int nx = i % Gm::NX, t = i / Gm::NX;
+        int c = t & 3, y = t >> 2;
+        float4 w = W[y % G];
+        int cy = y / G;
+        const float4 *n0 = Nd + (c * Gm::NY + cy) * Gm::NX + nx;
+        float4 a = n0[0], b = n0[Gm::NX], e = n0[2 * Gm::NX], f = n0[3 * Gm::NX];
+        float4 r;
+        r.x = fmaf(w.x, a.x, fmaf(w.y, b.x, fmaf(w.z, e.x, w.w * f.x)));
+        r.y = fmaf(w.x, a.y, fmaf(w.y, b.y, fmaf(w.z, e.y, w.w * f.y)));
+        r.z = fmaf(w.x, a.z, fmaf(w.y, b.z, fmaf(w.z, e.z, w.w * f.z)));
+        r.w = 0.f;
+        R[i] = r;
+    }
+    __syncthreads();
+
+    // per-thread x weights for its 8-voxel run (brick x origin is a multiple of G)
+    const int xrun = tx * kV;
+    const int cxt = xrun / G;
+    float4 wx[kV];
+#pragma unroll
+    for (int i = 0; i < kV; ++i) wx[i] = W[(xrun + i) % G];
+
+    const T *src = static_cast<const T *>(J.src);
+    T *dst = static_cast<T *>(J.dst);
+    const int64_t sbase = (O[2] - J.src_o[2]) * J.src_pz + (O[1] - J.src_o[1]) * J.src_py + (O[0] - J.src_o[0]);
+    const T *base = src + sbase;
+    const int py32 = (int)J.src_py, pz32 = (int)J.src_pz;
+    const int64_t dbase0 = (O[2] - J.out_o[2]) * J.dst_pz + (O[1] - J.out_o[1]) * J.dst_py + (O[0] - J.out_o[0]);
+    const bool vec = fast && ((((uintptr_t)J.dst) & 15) == 0) && ((J.dst_py * (int64_t)sizeof(T)) % 16 == 0) &&
+                     ((J.dst_pz * (int64_t)sizeof(T)) % 16 == 0) && ((dbase0 * (int64_t)sizeof(T)) % 16 == 0);
+    const int64_t xe = J.out_o[0] + J.out_n[0] - O[0];  // valid x extent in this brick
+    const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
+    const int64_t ze = J.out_o[2] + J.out_n[2] - O[2];
+
+    for (int z = 0; z < Gm::BZ; ++z) {
+        float4 *Q = Qb + (z & 1) * (Gm::BY * Gm::NX);
+        const float4 wz = W[z];
+        for (int i = tid; i < Gm::BY * Gm::NX; i += kThreads) {
+            int nx = i % Gm::NX, y = i / Gm::NX;
+            const float4 *r = R + (y * 4) * Gm::NX + nx;
+            float4 a = r[0], b = r[Gm::NX], e = r[2 * Gm::NX], f = r[3 * Gm::NX];
+            float4 q;
+            q.x = fmaf(wz.x, a.x, fmaf(wz.y, b.x, fmaf(wz.z, e.x, wz.w * f.x)));
+            q.y = fmaf(wz.x, a.y, fmaf(wz.y, b.y, fmaf(wz.z, e.y, wz.w * f.y)));
+            q.z = fmaf(wz.x, a.z, fmaf(wz.y, b.z, fmaf(wz.z, e.z, wz.w * f.z)));
+            q.w = 0.f;
+            Q[i] = q;
+        }
+        __syncthreads();
+        if (z >= ze) continue;  // uniform: whole slice outside the region
+#pragma unroll 1
+        for (int k = 0; k < Gm::ROWS; ++k) {
+            const int y = ty + kTY * k;
+            if (y >= ye) continue;
+            float4 qn[Gm::NT];
+#pragma unroll
+            for (int a = 0; a < Gm::NT; ++a) qn[a] = Q[y * Gm::NX + cxt + a];
+            uint32_t outv[kV];
+#pragma unroll
+            for (int i = 0; i < kV; ++i) {
+                // the run starts on a multiple of 8 and G divides 8 or 8 divides G, so the
+                // cell offset of voxel i within the run is a compile-time constant
+                const int ci = (G >= kV) ? 0 : (i / G);
+                const float4 w = wx[i];
+                float qx = fmaf(w.x, qn[ci].x, fmaf(w.y, qn[ci + 1].x, fmaf(w.z, qn[ci + 2].x, w.w * qn[ci + 3].x)));
+                float qy = fmaf(w.x, qn[ci].y, fmaf(w.y, qn[ci + 1].y, fmaf(w.z, qn[ci + 2].y, w.w * qn[ci + 3].y)));
+                float qz = fmaf(w.x, qn[ci].z, fmaf(w.y, qn[ci + 1].z, fmaf(w.z, qn[ci + 2].z, w.w * qn[ci + 3].z)));
+                float v;
+                if (fast) {
+                    v = sample_fast<T, INTERP>(base, py32, pz32, qx, qy, qz);
+                    outv[i] = INTERP == 1 ? (uint32_t)v : to_out<T, true>(v);
+                } else {
+                    bool ok = (xrun + i) < xe && sample_slow<T, INTERP>(J, O, qx, qy, qz, v);
+                    outv[i] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, true>(v)) : 0u;
+                }
+            }
+            T *drow = dst + dbase0 + (int64_t)z * J.dst_pz + (int64_t)y * J.dst_py + xrun;
+            int nvalid = (int)(xe - xrun);
+            if (nvalid > 0) store_run<T>(drow, outv, vec, nvalid > kV ? kV : nvalid);
+        }
+    }
+    __syncthreads();  // smem reuse by the next brick
+}
+
+// ---------------------------------------------------------------- affine
+
+constexpr int kABY = 8, kABZ = 8;
+
+template <typename T, int INTERP>
+__device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, float *red)
+{
+    const int tid = threadIdx.x;
+    const int tx = tid & 31, ty = tid >> 5;
+    const int64_t O[3] = {J.out_o[0] + bx * kBX, J.out_o[1] + by * kABY, J.out_o[2] + bz * kABZ};
+    // q(O + l) = M (O + l) = qO + Mlin l  (FP64 at the origin, FP32 increments)
+    double qO[3];
+    for (int r = 0; r < 3; ++r)
+        qO[r] = J.M[r * 4 + 0] * (double)O[0] + J.M[r * 4 + 1] * (double)O[1] + J.M[r * 4 + 2] * (double)O[2] +
+                J.M[r * 4 + 3];
+    // hull over the brick corners, relative to floor(qO)
+    int64_t qf[3];
+    float fo[3];
+    float lo[3], hi[3];
+    for (int r = 0; r < 3; ++r) {
+        double f = floor(qO[r]);
+        qf[r] = (int64_t)f;
+        fo[r] = (float)(qO[r] - f);
+        double l = 0, h = 0;
+        const double ext[3] = {kBX - 1.0, kABY - 1.0, kABZ - 1.0};
+        for (int a = 0; a < 3; ++a) {
+            double v = J.M[r * 4 + a] * ext[a];
+            if (v < 0) l += v; else h += v;
+        }
+        lo[r] = (float)(fo[r] + l);
+        hi[r] = (float)(fo[r] + h);
+    }
+    (void)red;
+    const bool inside_out = (O[0] + kBX <= J.out_o[0] + J.out_n[0]) && (O[1] + kABY <= J.out_o[1] + J.out_n[1]) &&
+                            (O[2] + kABZ <= J.out_o[2] + J.out_n[2]);
+    const bool fast = inside_out && hull_inside(J, qf, lo, hi);
+    const float m[3][3] = {{(float)J.M[0], (float)J.M[1], (float)J.M[2]},
+                           {(float)J.M[4], (float)J.M[5], (float)J.M[6]},
+                           {(float)J.M[8], (float)J.M[9], (float)J.M[10]}};
+    const T *src = static_cast<const T *>(J.src);
+    T *dst = static_cast<T *>(J.dst);
+    const int64_t sbase = (qf[2] - J.src_o[2]) * J.src_pz + (qf[1] - J.src_o[1]) * J.src_py + (qf[0] - J.src_o[0]);
+    const T *base = fast ? src + sbase : src;
+    const int py32 = (int)J.src_py, pz32 = (int)J.src_pz;
+    const int64_t dbase0 = (O[2] - J.out_o[2]) * J.dst_pz + (O[1] - J.out_o[1]) * J.dst_py + (O[0] - J.out_o[0]);
+    const bool vec = fast && ((((uintptr_t)J.dst) & 15) == 0) && ((J.dst_py * (int64_t)sizeof(T)) % 16 == 0) &&
+                     ((J.dst_pz * (int64_t)sizeof(T)) % 16 == 0) && ((dbase0 * (int64_t)sizeof(T)) % 16 == 0);
+    const int64_t xe = J.out_o[0] + J.out_n[0] - O[0];
+    const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
+    const int64_t ze = J.out_o[2] + J.out_n[2] - O[2];
+    const int xrun = tx * kV;
+    for (int z = 0; z < kABZ; ++z) {
+        if (z >= ze) break;
+        const int y = ty;
+        if (y >= ye) continue;
+        uint32_t outv[kV];
+        const float bx0 = fo[0] + m[0][1] * (float)y + m[0][2] * (float)z;
+        const float by0 = fo[1] + m[1][1] * (float)y + m[1][2] * (float)z;
+        const float bz0 = fo[2] + m[2][1] * (float)y + m[2][2] * (float)z;
+#pragma unroll
+        for (int i = 0; i < kV; ++i) {
+            const float lx = (float)(xrun + i);
+            float qx = fmaf(m[0][0], lx, bx0), qy = fmaf(m[1][0], lx, by0), qz = fmaf(m[2][0], lx, bz0);
+            float v;
+            if (fast) {
+                v = sample_fast<T, INTERP>(base, py32, pz32, qx, qy, qz);
+                outv[i] = INTERP == 1 ? (uint32_t)v : to_out<T, false>(v);
+            } else {
+                bool ok = (xrun + i) < xe && sample_slow<T, INTERP>(J, qf, qx, qy, qz, v);
+                outv[i] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, false>(v)) : 0u;
+            }
+        }
+        T *drow = dst + dbase0 + (int64_t)z * J.dst_pz + (int64_t)y * J.dst_py + xrun;
+        int nvalid = (int)(xe - xrun);
+        if (nvalid > 0) store_run<T>(drow, outv, vec, nvalid > kV ? kV : nvalid);
+    }
+}
+
+// ---------------------------------------------------------------- kernels
+
+template <typename T, int G, int INTERP>
+__global__ void __launch_bounds__(kThreads) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
+                                                            int64_t total_bricks)
+{
+    extern __shared__ float4 smem[];
+    __shared__ float red[6 * (kThreads / 32)];
+    using Gm = Geom<G>;
+    float4 *W = smem + Gm::UNION + Gm::NR;
+    if (threadIdx.x < G) W[threadIdx.x] = bspline_w(threadIdx.x, G);
+    __syncthreads();
+    for (int64_t b = blockIdx.x; b < total_bricks; b += gridDim.x) {
+        const int j = find_job(jobs, njobs, b);
+        const RJob &J = jobs[j];
+        int64_t lb = b - J.brick_begin;
+        int64_t bx = lb % J.bricks[0];
+        int64_t t = lb / J.bricks[0];
+        int64_t by = t % J.bricks[1];
+        int64_t bz = t / J.bricks[1];
+        tps_brick<T, G, INTERP>(J, bx, by, bz, smem, red);
+    }
+}
+
+template <typename T, int INTERP>
+__global__ void __launch_bounds__(kThreads) k_resample_affine(const RJob *__restrict__ jobs, int njobs,
+                                                               int64_t total_bricks)
+{
+    __shared__ float red[6 * (kThreads / 32)];
+    for (int64_t b = blockIdx.x; b < total_bricks; b += gridDim.x) {
+        const int j = find_job(jobs, njobs, b);
+        const RJob &J = jobs[j];
+        int64_t lb = b - J.brick_begin;
+        int64_t bx = lb % J.bricks[0];
+        int64_t t = lb / J.bricks[0];
+        int64_t by = t % J.bricks[1];
+        int64_t bz = t / J.bricks[1];
+        affine_brick<T, INTERP>(J, bx, by, bz, red);
+    }
+}
+
+template <typename T, int G, int INTERP>
+cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_t st, int sms)
+{
+    using Gm = Geom<G>;
+    auto k = k_resample_tps<T, G, INTERP>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, Gm::smem_bytes);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)sms * per_sm;
+    if (grid > total) grid = total;
+    if (grid < 1) grid = 1;
+    k<<<(unsigned)grid, kThreads, Gm::smem_bytes, st>>>(jobs, njobs, total);
+    return cudaGetLastError();
+}
+
+template <typename T, int INTERP>
+cudaError_t launch_affine_t(const RJob *jobs, int njobs, int64_t total, cudaStream_t st, int sms)
+{
+    auto k = k_resample_affine<T, INTERP>;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)sms * per_sm;
+    if (grid > total) grid = total;
+    if (grid < 1) grid = 1;
+    k<<<(unsigned)grid, kThreads, 0, st>>>(jobs, njobs, total);
+    return cudaGetLastError();
+}
+
+template <typename T, int INTERP>
+cudaError_t dispatch_g(const RJob *jobs, int njobs, int64_t total, int g, cudaStream_t st, int sms)
+{
+    switch (g) {
+    case 4: return launch_tps_t<T, 4, INTERP>(jobs, njobs, total, st, sms);
+    case 8: return launch_tps_t<T, 8, INTERP>(jobs, njobs, total, st, sms);
+    case 16: return launch_tps_t<T, 16, INTERP>(jobs, njobs, total, st, sms);
+    case 32: return launch_tps_t<T, 32, INTERP>(jobs, njobs, total, st, sms);
+    case 64: return launch_tps_t<T, 64, INTERP>(jobs, njobs, total, st, sms);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+bool g_supported(int g) { return g == 4 || g == 8 || g == 16 || g == 32 || g == 64; }
+
+void brick_dims(int kind, int g, int64_t out[3])
+{
+    if (kind == 0) {
+        out[0] = kBX; out[1] = kABY; out[2] = kABZ;
+        return;
+    }
+    out[0] = kBX;
+    out[1] = g < 8 ? 8 : g;
+    out[2] = g;
+}
+
+cudaError_t launch_resample(const RJob *jobs_dev, int njobs, int64_t total_bricks, int dtype, int kind, int g,
+                            int interp, cudaStream_t st, int sm_count)
+{
+    if (total_bricks <= 0) return cudaSuccess;
+    if (kind == 0) {
+        if (dtype == 1) return interp ? launch_affine_t<uint8_t, 1>(jobs_dev, njobs, total_bricks, st, sm_count)
+                                      : launch_affine_t<uint8_t, 0>(jobs_dev, njobs, total_bricks, st, sm_count);
+        return interp ? launch_affine_t<uint16_t, 1>(jobs_dev, njobs, total_bricks, st, sm_count)
+                      : launch_affine_t<uint16_t, 0>(jobs_dev, njobs, total_bricks, st, sm_count);
+    }
+    if (dtype == 1) return interp ? dispatch_g<uint8_t, 1>(jobs_dev, njobs, total_bricks, g, st, sm_count)
+                                  : dispatch_g<uint8_t, 0>(jobs_dev, njobs, total_bricks, g, st, sm_count);
+    return interp ? dispatch_g<uint16_t, 1>(jobs_dev, njobs, total_bricks, g, st, sm_count)
+                  : dispatch_g<uint16_t, 0>(jobs_dev, njobs, total_bricks, g, st, sm_count);
+}
+
+}  // namespace tw

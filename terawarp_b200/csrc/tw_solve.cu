@@ -1,0 +1,670 @@
+// tw_solve.cu -- FP64 landmark solves on sm_100a: the regularised TPS system
+// and the 3-D affine DLT fit.
+//
+// TPS (reference: compute_df_stps_subsampled_volume_4bspline,
+// q_imgwarp_tps_quicksmallmemory.cpp:377-588, whose GPU branch runs cuSOLVER
+// Sgeqrf on an N x N zero-padded copy of X (qr.cu:8-130), N-4 host round trips
+// of Gram-Schmidt (extendornormal.cu:55-150), four cublasSgemm calls with a
+// handle created per call (aff.cu:37-133) and an unpivoted FP32 Gauss-Jordan
+// inverse with 3(N-4) launches (GET_A_i.cu:80-161), all in FP32):
+//
+//   c = q2 (q2' K q2 + lambda I)^-1 q2' Y,   d = r^-1 q1' (Y - K c)
+//
+// is computed here entirely in FP64 without ever forming K, Q or A^-1:
+//   1. Householder QR of X = [1 s] (n x 4): 4 reflectors H_k = I - tau v v'.
+//      Q = H1 H2 H3 H4; q1 = Q(:,0:4), q2 = Q(:,4:n).  c and d do not depend
+//      on which orthonormal basis q2 is (the reference completes q1 by
+//      Gram-Schmidt instead), only on span(q2) = span(X)^perp.
+//   2. Q' K Q by four symmetric rank-2 updates: H K H = K - v w' - w v' with
+//      w = tau p - (tau^2 v'p / 2) v, p = K v.  All four p come from one
+//      product P0 = K V over the implicit K_ij = -|s_i - s_j|.
+//   3. A = (Q' K Q)(4:,4:) + lambda I is symmetric positive definite (-|r| is
+//      conditionally positive definite of order 1 in 3-D and q2 is orthogonal
+//      to the polynomials), so it is factored by a blocked right-looking
+//      Cholesky: diagonal block in shared memory, panel TRSM, trailing SYRK
+//      in 64 x 64 FP64 tiles.
+//   4. z = Q' Y; w = A^-1 z(4:) by forward/back substitution;
+//      c = Q [0; w]; d = R^-1 (Q' (Y - K c))(0:4).
+//
+// Affine (reference: q_affine_compute_affinmatrix_3D,
+// q_warp_affine_tps.cpp:649-731, newmat SVD of the 3N x 13 DLT matrix):
+// one CTA normalises both point sets, accumulates the 13 x 13 normal matrix
+// in FP64 and takes the eigenvector of its smallest eigenvalue by cyclic
+// Jacobi, which is the right singular vector the reference uses.
+
+#include "tw_internal.h"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace tw {
+
+namespace {
+
+constexpr int kNB = 64;          // Cholesky block
+constexpr int kRedThreads = 1024;
+
+// status word bits
+constexpr int kStSingularX = 1;
+constexpr int kStNotSPD = 2;
+
+__device__ double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < nw; ++i) t += sh[i];
+    return t;
+}
+
+__device__ __forceinline__ double kdist(const double *ctr, int i, int j)
+{
+    double dx = ctr[3 * i] - ctr[3 * j];
+    double dy = ctr[3 * i + 1] - ctr[3 * j + 1];
+    double dz = ctr[3 * i + 2] - ctr[3 * j + 2];
+    return -sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+// 1. Householder QR of X = [1 s].  Xw (n x 4) is a work copy; V (n x 4) gets
+// the reflectors (zeros above the diagonal), tau[4], R[16].
+__global__ void k_qr(const double *ctr, int n, double *Xw, double *V, double *tau, double *R, int *status)
+{
+    __shared__ double sh[32];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        Xw[i * 4 + 0] = 1.0;
+        Xw[i * 4 + 1] = ctr[3 * i];
+        Xw[i * 4 + 2] = ctr[3 * i + 1];
+        Xw[i * 4 + 3] = ctr[3 * i + 2];
+    }
+    __syncthreads();
+    double colnorm[4];
+    for (int j = 0; j < 4; ++j) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) s += Xw[i * 4 + j] * Xw[i * 4 + j];
+        colnorm[j] = sqrt(block_sum(s, sh));
+    }
+    for (int k = 0; k < 4; ++k) {
+        double s = 0.0;
+        for (int i = k + threadIdx.x; i < n; i += blockDim.x) s += Xw[i * 4 + k] * Xw[i * 4 + k];
+        const double nrm2 = block_sum(s, sh);
+        const double nrm = sqrt(nrm2);
+        const double xkk = Xw[k * 4 + k];
+        const double alpha = xkk > 0 ? -nrm : nrm;
+        const double vk = xkk - alpha;
+        const double vv = nrm2 - xkk * xkk + vk * vk;
+        const double t = vv > 0 ? 2.0 / vv : 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            V[i * 4 + k] = i < k ? 0.0 : (i == k ? vk : Xw[i * 4 + k]);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tau[k] = t;
+            R[k * 4 + k] = alpha;
+            for (int j = 0; j < k; ++j) R[k * 4 + j] = 0.0;
+            if (!(fabs(alpha) > 1e-10 * (colnorm[k] + 1e-300))) atomicOr(status, kStSingularX);
+        }
+        for (int j = k; j < 4; ++j) {
+            double d = 0.0;
+            for (int i = k + threadIdx.x; i < n; i += blockDim.x) d += V[i * 4 + k] * Xw[i * 4 + j];
+            const double sj = t * block_sum(d, sh);
+            for (int i = k + threadIdx.x; i < n; i += blockDim.x) Xw[i * 4 + j] -= sj * V[i * 4 + k];
+            __syncthreads();
+            if (threadIdx.x == 0 && j > k) R[k * 4 + j] = Xw[k * 4 + j];
+        }
+        __syncthreads();
+    }
+}
+
+// out (n x 4) = K B for the implicit K_ij = -|s_i - s_j|; one warp per row.
+__global__ void k_kmul(const double *ctr, int n, const double *B, double *out)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (int j = lane; j < n; j += 32) {
+        const double k = kdist(ctr, warp, j);
+        a0 += k * B[j * 4 + 0];
+        a1 += k * B[j * 4 + 1];
+        a2 += k * B[j * 4 + 2];
+        a3 += k * B[j * 4 + 3];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+    }
+    if (lane == 0) {
+        out[warp * 4 + 0] = a0;
+        out[warp * 4 + 1] = a1;
+        out[warp * 4 + 2] = a2;
+        out[warp * 4 + 3] = a3;
+    }
+}
+
+// 2. From P0 = K V derive the rank-2 update vectors W (n x 4), and Z = Q' Y.
+__global__ void k_wvec(int n, const double *V, const double *tau, const double *P0, double *W, const double *Y,
+                       double *Z)
+{
+    __shared__ double sh[32];
+    __shared__ double wv[4][4], vvd[4][4];  // w_j . v_k, v_j . v_k
+    for (int k = 0; k < 4; ++k) {
+        // p_k = P0_k - sum_{j<k} [ v_j (w_j . v_k) + w_j (v_j . v_k) ]
+        for (int j = 0; j < k; ++j) {
+            double a = 0, b = 0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                a += W[i * 4 + j] * V[i * 4 + k];
+                b += V[i * 4 + j] * V[i * 4 + k];
+            }
+            a = block_sum(a, sh);
+            b = block_sum(b, sh);
+            if (threadIdx.x == 0) { wv[j][k] = a; vvd[j][k] = b; }
+        }
+        __syncthreads();
+        double beta = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double p = P0[i * 4 + k];
+            for (int j = 0; j < k; ++j) p -= V[i * 4 + j] * wv[j][k] + W[i * 4 + j] * vvd[j][k];
+            W[i * 4 + k] = p;  // temporarily p
+            beta += V[i * 4 + k] * p;
+        }
+        beta = block_sum(beta, sh);
+        const double t = tau[k];
+        const double cf = 0.5 * t * t * beta;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) W[i * 4 + k] = t * W[i * 4 + k] - cf * V[i * 4 + k];
+        __syncthreads();
+    }
+    // Z = H4 H3 H2 H1 Y
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int c = 0; c < 4; ++c) Z[i * 4 + c] = Y[i * 4 + c];
+    __syncthreads();
+    for (int k = 0; k < 4; ++k) {
+        for (int c = 0; c < 4; ++c) {
+            double d = 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) d += V[i * 4 + k] * Z[i * 4 + c];
+            d = tau[k] * block_sum(d, sh);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) Z[i * 4 + c] -= d * V[i * 4 + k];
+            __syncthreads();
+        }
+    }
+}
+
+// 3a. A (m x m, row-major) = (Q'KQ)(4:,4:) + lambda I
+__global__ void k_fill_a(const double *ctr, int n, const double *V, const double *W, double lambda, double *A)
+{
+    const int m = n - 4;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= m || j >= m) return;
+    const int gi = i + 4, gj = j + 4;
+    double v = kdist(ctr, gi, gj);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v -= V[gi * 4 + k] * W[gj * 4 + k] + W[gi * 4 + k] * V[gj * 4 + k];
+    if (i == j) v += lambda;
+    A[(size_t)i * m + j] = v;
+}
+
+// 3b. factor the diagonal block kb in shared memory
+__global__ void k_potrf(double *A, int m, int kb, int *status)
+{
+    __shared__ double a[kNB][kNB + 1];
+    const int r0 = kb * kNB;
+    const int nb = min(kNB, m - r0);
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int r = e / kNB, c = e % kNB;
+        a[r][c] = (r < nb && c < nb) ? A[(size_t)(r0 + r) * m + r0 + c] : (r == c ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    for (int j = 0; j < kNB; ++j) {
+        if (threadIdx.x == 0) {
+            double d = a[j][j];
+            if (!(d > 0.0)) {
+                atomicOr(status, kStNotSPD);
+                d = 1.0;
+            }
+            a[j][j] = sqrt(d);
+        }
+        __syncthreads();
+        const double djj = a[j][j];
+        for (int i = j + 1 + threadIdx.x; i < kNB; i += blockDim.x) a[i][j] /= djj;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+            int i = e / kNB, l = e % kNB;
+            if (l > j && i >= l) a[i][l] -= a[i][j] * a[l][j];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int r = e / kNB, c = e % kNB;
+        if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c <= r ? a[r][c] : 0.0;
+    }
+}
+
+// 3c. panel: L(ib,kb) = A(ib,kb) L(kb,kb)^-T for all ib > kb; one CTA per
+// row block, one thread per row.
+__global__ void k_trsm(double *A, int m, int kb)
+{
+    extern __shared__ double dsm[];
+    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm);
+    double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm + kNB * (kNB + 1));
+    const int r0 = kb * kNB;
+    const int ib = kb + 1 + blockIdx.x;
+    const int i0 = ib * kNB;
+    const int nbk = min(kNB, m - r0);
+    const int nbi = min(kNB, m - i0);
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int r = e / kNB, c = e % kNB;
+        L[r][c] = (r < nbk && c < nbk) ? A[(size_t)(r0 + r) * m + r0 + c] : (r == c ? 1.0 : 0.0);
+        X[r][c] = (r < nbi && c < nbk) ? A[(size_t)(i0 + r) * m + r0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x;
+    if (r < nbi) {
+        for (int c = 0; c < nbk; ++c) {
+            double s = X[r][c];
+            for (int p = 0; p < c; ++p) s -= X[r][p] * L[c][p];
+            X[r][c] = s / L[c][c];
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int rr = e / kNB, c = e % kNB;
+        if (rr < nbi && c < nbk) A[(size_t)(i0 + rr) * m + r0 + c] = X[rr][c];
+    }
+}
+
+// 3d. trailing update A(ib,jb) -= L(ib,kb) L(jb,kb)' for kb < jb <= ib.
+// blockIdx.x enumerates the lower-triangular block pairs of the trailing
+// matrix; 256 threads, each owning a 4 x 4 patch of the 64 x 64 tile.
+__global__ void __launch_bounds__(256) k_syrk(double *A, int m, int kb)
+{
+    extern __shared__ double dsm[];
+    double(*Li)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm);
+    double(*Lj)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm + kNB * (kNB + 1));
+    // invert t = ib'(ib'+1)/2 + jb' (0 <= jb' <= ib')
+    const long long t = blockIdx.x;
+    int ibp = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((long long)(ibp + 1) * (ibp + 2) / 2 <= t) ++ibp;
+    while ((long long)ibp * (ibp + 1) / 2 > t) --ibp;
+    const int jbp = (int)(t - (long long)ibp * (ibp + 1) / 2);
+    const int ib = kb + 1 + ibp, jb = kb + 1 + jbp;
+    const int r0 = kb * kNB, i0 = ib * kNB, j0 = jb * kNB;
+    const int nbk = min(kNB, m - r0), nbi = min(kNB, m - i0), nbj = min(kNB, m - j0);
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int r = e / kNB, c = e % kNB;
+        Li[r][c] = (r < nbi && c < nbk) ? A[(size_t)(i0 + r) * m + r0 + c] : 0.0;
+        Lj[r][c] = (r < nbj && c < nbk) ? A[(size_t)(j0 + r) * m + r0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int tr = (threadIdx.x / 16) * 4, tc = (threadIdx.x % 16) * 4;
+    double acc[4][4] = {};
+    for (int p = 0; p < nbk; ++p) {
+        double a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = Li[tr + u][p];
+            b[u] = Lj[tc + u][p];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            int r = tr + u, c = tc + v;
+            if (r < nbi && c < nbj && (ib != jb || c <= r)) A[(size_t)(i0 + r) * m + j0 + c] -= acc[u][v];
+        }
+}
+
+// 4a. forward substitution L y = z(4:) for 4 right-hand sides, in place in
+// Z rows 4..n-1.  One CTA of 1024 threads.
+__global__ void k_fwd(const double *A, int m, double *Z)
+{
+    __shared__ double y[kNB][4];
+    double *z = Z + 16;  // rows 4.. of the n x 4 Z
+    for (int kb = 0; kb * kNB < m; ++kb) {
+        const int r0 = kb * kNB, nb = min(kNB, m - r0);
+        // diagonal block: warp c handles right-hand side c
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (warp < 4) {
+            for (int r = 0; r < nb; ++r) {
+                double s = 0.0;
+                for (int p = lane; p < r; p += 32) s += A[(size_t)(r0 + r) * m + r0 + p] * y[p][warp];
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) y[r][warp] = (z[(r0 + r) * 4 + warp] - s) / A[(size_t)(r0 + r) * m + r0 + r];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < nb * 4; r += blockDim.x) z[(r0 + r / 4) * 4 + (r % 4)] = y[r / 4][r % 4];
+        // update the rows below
+        for (int i = r0 + nb + threadIdx.x; i < m; i += blockDim.x) {
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+            const double *Li = A + (size_t)i * m + r0;
+            for (int p = 0; p < nb; ++p) {
+                const double l = Li[p];
+                s0 += l * y[p][0]; s1 += l * y[p][1]; s2 += l * y[p][2]; s3 += l * y[p][3];
+            }
+            z[i * 4 + 0] -= s0; z[i * 4 + 1] -= s1; z[i * 4 + 2] -= s2; z[i * 4 + 3] -= s3;
+        }
+        __syncthreads();
+    }
+}
+
+// 4b. back substitution L' x = y, in place.
+__global__ void k_bwd(const double *A, int m, double *Z)
+{
+    __shared__ double x[kNB][4];
+    double *z = Z + 16;
+    const int nblk = (m + kNB - 1) / kNB;
+    for (int kb = nblk - 1; kb >= 0; --kb) {
+        const int r0 = kb * kNB, nb = min(kNB, m - r0);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (warp < 4) {
+            for (int r = nb - 1; r >= 0; --r) {
+                double s = 0.0;
+                for (int p = r + 1 + lane; p < nb; p += 32) s += A[(size_t)(r0 + p) * m + r0 + r] * x[p][warp];
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) x[r][warp] = (z[(r0 + r) * 4 + warp] - s) / A[(size_t)(r0 + r) * m + r0 + r];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < nb * 4; r += blockDim.x) z[(r0 + r / 4) * 4 + (r % 4)] = x[r / 4][r % 4];
+        for (int i = threadIdx.x; i < r0; i += blockDim.x) {
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+            for (int p = 0; p < nb; ++p) {
+                const double l = A[(size_t)(r0 + p) * m + i];
+                s0 += l * x[p][0]; s1 += l * x[p][1]; s2 += l * x[p][2]; s3 += l * x[p][3];
+            }
+            z[i * 4 + 0] -= s0; z[i * 4 + 1] -= s1; z[i * 4 + 2] -= s2; z[i * 4 + 3] -= s3;
+        }
+        __syncthreads();
+    }
+}
+
+// 4c. c = H1 H2 H3 H4 [0; w]  (Z rows 0..3 are replaced by zeros)
+__global__ void k_apply_q(int n, const double *V, const double *tau, const double *Z, double *C)
+{
+    __shared__ double sh[32];
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int c = 0; c < 4; ++c) C[i * 4 + c] = i < 4 ? 0.0 : Z[i * 4 + c];
+    __syncthreads();
+    for (int k = 3; k >= 0; --k) {
+        for (int c = 0; c < 4; ++c) {
+            double d = 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) d += V[i * 4 + k] * C[i * 4 + c];
+            d = tau[k] * block_sum(d, sh);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) C[i * 4 + c] -= d * V[i * 4 + k];
+            __syncthreads();
+        }
+    }
+}
+
+// 4d. d = R^-1 (Q' (Y - K c))(0:4); KC = K c precomputed.
+__global__ void k_finish_d(int n, const double *V, const double *tau, const double *R, const double *Y, double *KC,
+                           double *d_out)
+{
+    __shared__ double sh[32];
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int c = 0; c < 4; ++c) KC[i * 4 + c] = Y[i * 4 + c] - KC[i * 4 + c];
+    __syncthreads();
+    for (int k = 0; k < 4; ++k) {
+        for (int c = 0; c < 4; ++c) {
+            double d = 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) d += V[i * 4 + k] * KC[i * 4 + c];
+            d = tau[k] * block_sum(d, sh);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) KC[i * 4 + c] -= d * V[i * 4 + k];
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 4; ++c)
+            for (int a = 3; a >= 0; --a) {
+                double s = KC[a * 4 + c];
+                for (int b = a + 1; b < 4; ++b) s -= R[a * 4 + b] * d_out[b * 4 + c];
+                d_out[a * 4 + c] = s / R[a * 4 + a];
+            }
+    }
+}
+
+// ----------------------------------------------------------- affine DLT
+
+__global__ void k_affine_fit(const double *tar, const double *sub, int n, double *out, int *status)
+{
+    __shared__ double sh[32];
+    __shared__ double ata[13][13];
+    __shared__ double nrm[2][4];  // scale, cx, cy, cz for A (tar) and B (sub)
+    for (int s = 0; s < 2; ++s) {
+        const double *p = s == 0 ? tar : sub;
+        double cx = 0, cy = 0, cz = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) { cx += p[3 * i]; cy += p[3 * i + 1]; cz += p[3 * i + 2]; }
+        cx = block_sum(cx, sh) / n;
+        cy = block_sum(cy, sh) / n;
+        cz = block_sum(cz, sh) / n;
+        double dsum = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double dx = p[3 * i] - cx, dy = p[3 * i + 1] - cy, dz = p[3 * i + 2] - cz;
+            dsum += sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        dsum = block_sum(dsum, sh) / n;
+        if (threadIdx.x == 0) { nrm[s][0] = 1.0 / dsum; nrm[s][1] = cx; nrm[s][2] = cy; nrm[s][3] = cz; }
+        __syncthreads();
+    }
+    // normal matrix of the 3n x 13 DLT system, row block per point:
+    // [a 1 0 0 -bx], [0 a 1 0 -by], [0 0 a 1 -bz] with a = (ax, ay, az)
+    for (int e = 0; e < 169; ++e) {
+        const int r = e / 13, c = e % 13;
+        if (c < r) continue;
+        double acc = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double a[3], b[3];
+            for (int q = 0; q < 3; ++q) {
+                a[q] = (tar[3 * i + q] - nrm[0][1 + q]) * nrm[0][0];
+                b[q] = (sub[3 * i + q] - nrm[1][1 + q]) * nrm[1][0];
+            }
+            for (int rb = 0; rb < 3; ++rb) {
+                double row[13] = {0};
+                row[rb * 4 + 0] = a[0]; row[rb * 4 + 1] = a[1]; row[rb * 4 + 2] = a[2]; row[rb * 4 + 3] = 1.0;
+                row[12] = -b[rb];
+                acc += row[r] * row[c];
+            }
+        }
+        acc = block_sum(acc, sh);
+        if (threadIdx.x == 0) { ata[r][c] = acc; ata[c][r] = acc; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double Vm[13][13];
+        for (int i = 0; i < 13; ++i)
+            for (int j = 0; j < 13; ++j) Vm[i][j] = i == j ? 1.0 : 0.0;
+        for (int sweep = 0; sweep < 100; ++sweep) {
+            double off = 0, diag = 0;
+            for (int p = 0; p < 13; ++p) {
+                diag += ata[p][p] * ata[p][p];
+                for (int q = p + 1; q < 13; ++q) off += ata[p][q] * ata[p][q];
+            }
+            if (off <= 1e-30 * diag) break;
+            for (int p = 0; p < 12; ++p)
+                for (int q = p + 1; q < 13; ++q) {
+                    double apq = ata[p][q];
+                    if (fabs(apq) < 1e-300) continue;
+                    double theta = (ata[q][q] - ata[p][p]) / (2.0 * apq);
+                    double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                    double cs = 1.0 / sqrt(t * t + 1.0), sn = t * cs;
+                    for (int k = 0; k < 13; ++k) {
+                        double akp = ata[k][p], akq = ata[k][q];
+                        ata[k][p] = cs * akp - sn * akq;
+                        ata[k][q] = sn * akp + cs * akq;
+                    }
+                    for (int k = 0; k < 13; ++k) {
+                        double apk = ata[p][k], aqk = ata[q][k];
+                        ata[p][k] = cs * apk - sn * aqk;
+                        ata[q][k] = sn * apk + cs * aqk;
+                    }
+                    for (int k = 0; k < 13; ++k) {
+                        double vkp = Vm[k][p], vkq = Vm[k][q];
+                        Vm[k][p] = cs * vkp - sn * vkq;
+                        Vm[k][q] = sn * vkp + cs * vkq;
+                    }
+                }
+        }
+        int best = 0;
+        for (int p = 1; p < 13; ++p)
+            if (ata[p][p] < ata[best][best]) best = p;
+        double h[13];
+        for (int i = 0; i < 13; ++i) h[i] = Vm[i][best];
+        if (h[12] == 0.0) {
+            atomicOr(status, kStSingularX);
+            return;
+        }
+        for (int i = 0; i < 13; ++i) h[i] /= h[12];
+        // T = NB^-1 H NA with N = [s I, -s c; 0 1]:  NB^-1 = [I/sB, cB; 0 1]
+        const double sA = nrm[0][0], sB = nrm[1][0];
+        double H[3][4];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) H[r][c] = h[r * 4 + c];
+        for (int r = 0; r < 3; ++r) {
+            // (H NA)(r,:) = [sA H(r,0:3), H(r,3) - sA H(r,0:3).cA]
+            double lin[3], tr = H[r][3];
+            for (int c = 0; c < 3; ++c) {
+                lin[c] = sA * H[r][c];
+                tr -= sA * H[r][c] * nrm[0][1 + c];
+            }
+            for (int c = 0; c < 3; ++c) out[r * 4 + c] = lin[c] / sB;
+            out[r * 4 + 3] = tr / sB + nrm[1][1 + r];
+        }
+        out[12] = 0; out[13] = 0; out[14] = 0; out[15] = 1;
+    }
+}
+
+struct DevBuf {
+    tw_ctx *ctx = nullptr;
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { if (p) dfree(ctx, p, bytes); }
+};
+
+}  // namespace
+
+tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
+                           double *d_c_out, double *h_d_out, cudaStream_t st)
+{
+    const int m = n - 4;
+    // workspace: ctr 3n, Y 4n, Xw 4n, V 4n, P 4n, W 4n, Z 4n, KC 4n, tau 4, R 16, d 16, status
+    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + 16 + 2;
+    DevBuf ws{ctx}, abuf{ctx};
+    ws.bytes = small * sizeof(double);
+    TW_TRY(dmalloc(ctx, &ws.p, ws.bytes));
+    double *base = static_cast<double *>(ws.p);
+    double *d_ctr = base;
+    double *d_Y = d_ctr + 3 * (size_t)n;
+    double *d_Xw = d_Y + 4 * (size_t)n;
+    double *d_V = d_Xw + 4 * (size_t)n;
+    double *d_P = d_V + 4 * (size_t)n;
+    double *d_W = d_P + 4 * (size_t)n;
+    double *d_Z = d_W + 4 * (size_t)n;
+    double *d_KC = d_Z + 4 * (size_t)n;
+    double *d_tau = d_KC + 4 * (size_t)n;
+    double *d_R = d_tau + 4;
+    double *d_d = d_R + 16;
+    int *d_status = reinterpret_cast<int *>(d_d + 16);
+    if (m > 0) {
+        abuf.bytes = (size_t)m * m * sizeof(double);
+        TW_TRY(dmalloc(ctx, &abuf.p, abuf.bytes));
+    }
+    double *d_A = static_cast<double *>(abuf.p);
+
+    std::vector<double> hY(4 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        hY[4 * i + 0] = 1.0;
+        hY[4 * i + 1] = h_val[3 * i + 0];
+        hY[4 * i + 2] = h_val[3 * i + 1];
+        hY[4 * i + 3] = h_val[3 * i + 2];
+    }
+    TW_CUDA_TRY(cudaMemcpyAsync(d_ctr, h_ctr, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaMemcpyAsync(d_Y, hY.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    TW_CUDA_TRY(cudaMemsetAsync(d_d, 0, sizeof(double) * 16, st));
+
+    uint64_t nl = 0;
+    k_qr<<<1, kRedThreads, 0, st>>>(d_ctr, n, d_Xw, d_V, d_tau, d_R, d_status);
+    ++nl;
+    const int warps_per_block = 8;
+    const unsigned kgrid = (unsigned)((n + warps_per_block - 1) / warps_per_block);
+    k_kmul<<<kgrid, 32 * warps_per_block, 0, st>>>(d_ctr, n, d_V, d_P);
+    k_wvec<<<1, kRedThreads, 0, st>>>(n, d_V, d_tau, d_P, d_W, d_Y, d_Z);
+    nl += 2;
+    if (m > 0) {
+        dim3 b(32, 8), g((m + 31) / 32, (m + 7) / 8);
+        k_fill_a<<<g, b, 0, st>>>(d_ctr, n, d_V, d_W, lambda, d_A);
+        ++nl;
+        const int nblk = (m + kNB - 1) / kNB;
+        const int tile_smem = (int)(2 * sizeof(double) * kNB * (kNB + 1));
+        TW_CUDA_TRY(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
+        TW_CUDA_TRY(cudaFuncSetAttribute(k_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
+        for (int kb = 0; kb < nblk; ++kb) {
+            k_potrf<<<1, 256, 0, st>>>(d_A, m, kb, d_status);
+            ++nl;
+            const int rest = nblk - kb - 1;
+            if (rest > 0) {
+                k_trsm<<<rest, kNB, tile_smem, st>>>(d_A, m, kb);
+                const long long pairs = (long long)rest * (rest + 1) / 2;
+                k_syrk<<<(unsigned)pairs, 256, tile_smem, st>>>(d_A, m, kb);
+                nl += 2;
+            }
+        }
+        k_fwd<<<1, kRedThreads, 0, st>>>(d_A, m, d_Z);
+        k_bwd<<<1, kRedThreads, 0, st>>>(d_A, m, d_Z);
+        nl += 2;
+    }
+    k_apply_q<<<1, kRedThreads, 0, st>>>(n, d_V, d_tau, d_Z, d_c_out);
+    k_kmul<<<kgrid, 32 * warps_per_block, 0, st>>>(d_ctr, n, d_c_out, d_KC);
+    k_finish_d<<<1, kRedThreads, 0, st>>>(n, d_V, d_tau, d_R, d_Y, d_KC, d_d);
+    nl += 3;
+    TW_CUDA_TRY(cudaGetLastError());
+    count_launch(ctx, nl);
+    int status = 0;
+    TW_CUDA_TRY(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TW_CUDA_TRY(cudaMemcpyAsync(h_d_out, d_d, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
+    TW_CUDA_TRY(cudaStreamSynchronize(st));
+    if (status & kStSingularX)
+        return fail(ctx, TW_ERR_SINGULAR, "TPS centres are degenerate: [1 s] is rank deficient (coplanar or < 4 distinct points)");
+    if (status & kStNotSPD)
+        return fail(ctx, TW_ERR_SINGULAR, "projected TPS system is not positive definite");
+    return TW_OK;
+}
+
+tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_sub, int n, double M[16],
+                            cudaStream_t st)
+{
+    DevBuf ws{ctx};
+    ws.bytes = sizeof(double) * (6 * (size_t)n + 16 + 2);
+    TW_TRY(dmalloc(ctx, &ws.p, ws.bytes));
+    double *d_tar = static_cast<double *>(ws.p);
+    double *d_sub = d_tar + 3 * (size_t)n;
+    double *d_out = d_sub + 3 * (size_t)n;
+    int *d_status = reinterpret_cast<int *>(d_out + 16);
+    TW_CUDA_TRY(cudaMemcpyAsync(d_tar, h_tar, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaMemcpyAsync(d_sub, h_sub, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    k_affine_fit<<<1, 256, 0, st>>>(d_tar, d_sub, n, d_out, d_status);
+    TW_CUDA_TRY(cudaGetLastError());
+    count_launch(ctx, 1);
+    int status = 0;
+    TW_CUDA_TRY(cudaMemcpyAsync(M, d_out, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
+    TW_CUDA_TRY(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TW_CUDA_TRY(cudaStreamSynchronize(st));
+    if (status) return fail(ctx, TW_ERR_SINGULAR, "affine DLT is degenerate (h13 = 0)");
+    return TW_OK;
+}
+
+}  // namespace tw

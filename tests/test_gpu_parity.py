@@ -1,0 +1,320 @@
+"""Parity of the sm_100a path (through the C ABI) with the FP64 oracle and the
+golden fixtures.
+
+Tolerances (from the task's precision pattern):
+  - solve: FP64 both sides, relative 1e-7 on c and d
+  - node displacement: <= 0.01 voxel max error vs FP64 (FP32 compensated eval)
+  - intensities: |diff| <= 1 level on >= 99.99% of voxels
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import terawarp_b200 as tw
+from oracle import oracle as O
+from terawarp_b200 import synth
+
+pytestmark = pytest.mark.gpu
+G = np.load(Path(__file__).resolve().parent / "golden" / "golden_small.npz")
+INT_TOL_FRAC = 0.9999
+
+
+def agree(a, b, frac=INT_TOL_FRAC):
+    d = np.abs(np.asarray(a, np.int64) - np.asarray(b, np.int64))
+    within = (d <= 1).mean()
+    assert within >= frac, f"only {within:.6f} of voxels within +-1 (max diff {d.max()})"
+    return d
+
+
+def landmarks(n, sz, seed, sigma=2.0, margin=3.0):
+    rng = np.random.default_rng(seed)
+    sub = rng.uniform(margin, np.array(sz) - 1 - margin, size=(n, 3)).astype(np.float32)
+    tar = (sub + rng.normal(0, sigma, size=sub.shape)).astype(np.float32)
+    return sub, tar
+
+
+def vol(shape_zyx, dtype, seed):
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 256 if dtype == np.uint8 else 4096, size=shape_zyx).astype(dtype)
+
+
+# ------------------------------------------------------------------ solve
+
+@pytest.mark.parametrize("n", [4, 5, 16, 64, 300, 1000])
+def test_solve_matches_oracle(ctx, n):
+    sub, tar = landmarks(n, (200, 180, 90), n)
+    t = tw.tps_solve(ctx, sub, tar)
+    c, d = t.coeffs()
+    c0, d0 = O.tps_solve(sub, tar)
+    scale_c = max(1.0, np.abs(c0).max())
+    np.testing.assert_allclose(c, c0, atol=1e-7 * scale_c)
+    np.testing.assert_allclose(d, d0, atol=1e-7 * max(1.0, np.abs(d0).max()))
+
+
+def test_solve_golden(ctx):
+    t = tw.tps_solve(ctx, G["tps_ctr"], G["tps_val"])
+    c, d = t.coeffs()
+    np.testing.assert_allclose(c, G["tps_c"], atol=1e-10)
+    np.testing.assert_allclose(d, G["tps_d"], atol=1e-9)
+
+
+def test_solve_rejects_coplanar_landmarks(ctx):
+    rng = np.random.default_rng(3)
+    p = rng.uniform(0, 50, size=(20, 3)).astype(np.float32)
+    p[:, 2] = 7.0  # all in one plane
+    with pytest.raises(tw.TeraWarpError) as e:
+        tw.tps_solve(ctx, p, p + 1)
+    assert e.value.status == 2
+
+
+def test_solve_rejects_too_few_points(ctx):
+    p = np.zeros((3, 3), np.float32)
+    with pytest.raises(tw.TeraWarpError):
+        tw.tps_solve(ctx, p, p)
+
+
+# ------------------------------------------------------------- node grid
+
+@pytest.mark.parametrize("g,n,sz", [(4, 12, (36, 30, 22)), (8, 64, (256, 256, 128)), (16, 500, (512, 512, 256)),
+                                    (16, 2000, (1024, 1024, 512))])
+def test_grid_eval_error_below_hundredth_voxel(ctx, g, n, sz):
+    if n >= 500:
+        sub, tar = synth.lattice_landmarks(sz, n, 11)
+    else:
+        sub, tar = landmarks(n, sz, 7, sigma=3.0)
+    t = tw.tps_solve(ctx, tar, sub)  # centres = target points, values = subject points
+    gsz = tuple(tw.grid_size(s, g) for s in sz)
+    nodes = tw.tps_eval_grid(ctx, t, gsz, g).cpu().numpy()[..., :3]
+    c, d = O.tps_solve(tar, sub)
+    ref = O.tps_grid(tar, c, d, gsz, g)
+    err = np.abs(nodes.astype(np.float64) - ref.astype(np.float64))
+    assert err.max() <= 0.01, err.max()
+    assert np.sqrt((err ** 2).mean()) <= 0.002
+
+
+@pytest.mark.parametrize("g", [4, 8])
+def test_grid_golden(ctx, g):
+    src = G["tps_src"]
+    Z, Y, X = src.shape
+    t = tw.tps_solve(ctx, G["tps_ctr"], G["tps_val"])
+    gsz = (tw.grid_size(X, g), tw.grid_size(Y, g), tw.grid_size(Z, g))
+    nodes = tw.tps_eval_grid(ctx, t, gsz, g).cpu().numpy()[..., :3]
+    np.testing.assert_allclose(nodes, G[f"tps_df_g{g}"], atol=2e-3)
+
+
+# ---------------------------------------------------- B-spline + resample
+
+def _warp_device(ctx, nodes_t, g, src_np, interp=0):
+    src = torch.from_numpy(src_np).cuda()
+    dst = torch.empty_like(src)
+    tw.warp_tps_device(ctx, nodes_t, g, src, dst, interp)
+    torch.cuda.synchronize()
+    return dst.cpu().numpy()
+
+
+@pytest.mark.parametrize("g", [4, 8, 16, 32, 64])
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
+@pytest.mark.parametrize("interp", [0, 1])
+def test_resample_matches_oracle_on_same_nodes(ctx, g, dtype, interp):
+    shape = (70, 100, 300) if g <= 16 else (140, 150, 300)
+    Z, Y, X = shape
+    src = vol(shape, dtype, g)
+    sub, tar = landmarks(24, (X, Y, Z), g + 1, sigma=3.0)
+    t = tw.tps_solve(ctx, tar, sub)
+    gsz = (tw.grid_size(X, g), tw.grid_size(Y, g), tw.grid_size(Z, g))
+    nodes = tw.tps_eval_grid(ctx, t, gsz, g)
+    out = _warp_device(ctx, nodes, g, src, interp)
+    ref = O.tps_warp(src, np.ascontiguousarray(nodes.cpu().numpy()[..., :3]), g, interp)
+    d = agree(out, ref)
+    assert (d == 0).mean() >= 0.999
+
+
+@pytest.mark.parametrize("shape", [(21, 37, 53), (9, 10, 11), (33, 64, 257), (16, 16, 16)])
+def test_resample_odd_sizes_and_edges(ctx, shape):
+    g = 4
+    Z, Y, X = shape
+    src = vol(shape, np.uint16, 5)
+    sub, tar = landmarks(8, (X, Y, Z), 2, sigma=2.5, margin=1.0)
+    t = tw.tps_solve(ctx, tar, sub)
+    gsz = (tw.grid_size(X, g), tw.grid_size(Y, g), tw.grid_size(Z, g))
+    nodes = tw.tps_eval_grid(ctx, t, gsz, g)
+    out = _warp_device(ctx, nodes, g, src)
+    ref = O.tps_warp(src, np.ascontiguousarray(nodes.cpu().numpy()[..., :3]), g)
+    agree(out, ref)
+
+
+def test_resample_large_displacement_out_of_bounds(ctx):
+    # targets pushed far from subjects: many samples leave the volume -> 0
+    g = 8
+    shape = (40, 64, 96)
+    Z, Y, X = shape
+    src = vol(shape, np.uint8, 9)
+    rng = np.random.default_rng(4)
+    sub = rng.uniform(0, [X, Y, Z], size=(20, 3)).astype(np.float32)
+    tar = (sub + rng.normal(0, 15, size=sub.shape)).astype(np.float32)
+    t = tw.tps_solve(ctx, tar, sub)
+    gsz = (tw.grid_size(X, g), tw.grid_size(Y, g), tw.grid_size(Z, g))
+    nodes = tw.tps_eval_grid(ctx, t, gsz, g)
+    out = _warp_device(ctx, nodes, g, src)
+    ref = O.tps_warp(src, np.ascontiguousarray(nodes.cpu().numpy()[..., :3]), g)
+    assert (ref == 0).mean() > 0.05
+    agree(out, ref)
+
+
+# ---------------------------------------------------------- full pipeline
+
+@pytest.mark.parametrize("g", [4, 16])
+def test_imgwarp_smallmemory_image_matches_oracle(ctx, g):
+    case = synth.plain_tps_case(device="cpu", shape_zyx=(64, 96, 128), n=32, g=g)
+    img = case.vol.numpy()
+    # reference call order: (ql_marker_tar, ql_marker_sub) <- plugin's (sub, tar)
+    out = tw.imgwarp_smallmemory_image(ctx, case.marker_sub, case.marker_tar, g, g, g, 1, 0, img)
+    ref = O.imgwarp_smallmemory_image(case.marker_sub, case.marker_tar, g, img)
+    d = agree(out, ref)
+    assert (d == 0).mean() >= 0.999
+
+
+def test_plain_tps_full_size(ctx):
+    """The plain TPS workload at full size: 256x256x128 uint8, 64 pairs, g=16."""
+    case = synth.plain_tps_case(device="cpu")
+    img = case.vol.numpy()
+    out = tw.imgwarp_smallmemory_image(ctx, case.marker_sub, case.marker_tar, 16, 16, 16, 1, 0, img)
+    ref = O.imgwarp_smallmemory_image(case.marker_sub, case.marker_tar, 16, img)
+    d = agree(out, ref)
+    assert (d == 0).mean() >= 0.999
+
+
+def test_golden_pipeline(ctx):
+    src = G["tps_src"]
+    out = tw.imgwarp_smallmemory_image(ctx, G["tps_val"], G["tps_ctr"], 4, 4, 4, 1, 0, src)
+    agree(out, G["tps_out_g4"], frac=0.999)
+
+
+def test_identity_landmarks_copy_interior(ctx):
+    src = vol((20, 24, 28), np.uint8, 0)
+    rng = np.random.default_rng(1)
+    pts = rng.uniform(2, 18, size=(10, 3)).astype(np.float32)
+    out = tw.imgwarp_smallmemory_image(ctx, pts, pts, 4, 4, 4, 1, 0, src)
+    np.testing.assert_array_equal(out[1:-1, 1:-1, 1:-1], src[1:-1, 1:-1, 1:-1])
+
+
+def test_multichannel_and_host_buffer_kinds(ctx):
+    case = synth.plain_tps_case(device="cpu", shape_zyx=(32, 48, 64), n=16, g=8)
+    one = case.vol.numpy()
+    img = np.stack([one, 255 - one])  # (c, z, y, x)
+    out_np = tw.imgwarp_smallmemory_image(ctx, case.marker_sub, case.marker_tar, 8, 8, 8, 1, 0, img)
+    pinned = torch.from_numpy(img).pin_memory()
+    out_pin = tw.imgwarp_smallmemory_image(ctx, case.marker_sub, case.marker_tar, 8, 8, 8, 1, 0, pinned)
+    dev = torch.from_numpy(img).cuda()
+    out_dev = tw.imgwarp_smallmemory_image(ctx, case.marker_sub, case.marker_tar, 8, 8, 8, 1, 0, dev)
+    np.testing.assert_array_equal(out_np, out_pin.numpy())
+    np.testing.assert_array_equal(out_np, out_dev.cpu().numpy())
+    ref0 = O.imgwarp_smallmemory_image(case.marker_sub, case.marker_tar, 8, img[0])
+    ref1 = O.imgwarp_smallmemory_image(case.marker_sub, case.marker_tar, 8, img[1])
+    agree(out_np[0], ref0)
+    agree(out_np[1], ref1)
+
+
+def test_reference_argument_checks(ctx):
+    img = vol((10, 12, 14), np.uint8, 0)
+    p = np.random.default_rng(0).uniform(1, 8, size=(6, 3)).astype(np.float32)
+    with pytest.raises(tw.TeraWarpError):  # block >= image size
+        tw.imgwarp_smallmemory_image(ctx, p, p, 16, 16, 16, 1, 0, img)
+    with pytest.raises(tw.TeraWarpError):  # unequal block sizes
+        tw.imgwarp_smallmemory_image(ctx, p, p, 4, 4, 8, 1, 0, img)
+    with pytest.raises(tw.TeraWarpError):  # interp method
+        tw.imgwarp_smallmemory_image(ctx, p, p, 4, 4, 4, 1, 2, img)
+
+
+# ----------------------------------------------------------------- affine
+
+def test_affine_fit_matches_oracle_and_golden(ctx):
+    M = tw.fit_affine(ctx, G["aff_tar"], G["aff_sub"])
+    np.testing.assert_allclose(M, G["aff_M"], atol=1e-8)
+    M2 = synth.random_affine(5, (300, 200, 100))
+    sub, tar = synth.affine_landmarks(M2, (300, 200, 100), 32, 6)
+    np.testing.assert_allclose(tw.fit_affine(ctx, tar, sub), O.affine_fit(tar, sub), atol=1e-8)
+
+
+def test_affine_golden_warp(ctx):
+    src = torch.from_numpy(G["aff_src"]).cuda()
+    dst = torch.empty((20, 24, 28), dtype=torch.uint16, device="cuda")
+    tw.warp_affine_device(ctx, G["aff_M"], src, dst)
+    torch.cuda.synchronize()
+    agree(dst.cpu().numpy(), G["aff_out"], frac=0.999)
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
+@pytest.mark.parametrize("interp", [0, 1])
+@pytest.mark.parametrize("out_shape", [(60, 90, 130), (47, 81, 301)])
+def test_affine_warp_matches_oracle(ctx, dtype, interp, out_shape):
+    shape = (60, 90, 130)
+    src_np = vol(shape, dtype, 3)
+    M = synth.random_affine(7, (130, 90, 60), trans=5.0)
+    src = torch.from_numpy(src_np).cuda()
+    dst = torch.empty(out_shape, dtype=src.dtype, device="cuda")
+    tw.warp_affine_device(ctx, M, src, dst, interp)
+    torch.cuda.synchronize()
+    ref = O.affine_warp(src_np, M, out_shape, interp)
+    d = agree(dst.cpu().numpy(), ref)
+    assert (d == 0).mean() >= 0.999
+
+
+def test_q_imagewarp_affine_image_matches_oracle(ctx):
+    case = synth.affine_case(device="cpu", shape_zyx=(48, 80, 96), n=32)
+    img = case.vol.numpy()
+    out = tw.q_imagewarp_affine_image(ctx, case.marker_tar, case.marker_sub, img)
+    M = O.affine_fit(case.marker_tar, case.marker_sub)
+    ref = O.affine_warp(img, M)
+    agree(out, ref)
+
+
+def test_integer_shift_is_exact(ctx):
+    src_np = vol((16, 18, 20), np.uint16, 1)
+    M = np.eye(4)
+    M[:3, 3] = [2, -1, 3]
+    src = torch.from_numpy(src_np).cuda()
+    dst = torch.empty_like(src)
+    tw.warp_affine_device(ctx, M, src, dst)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dst.cpu().numpy(), O.affine_warp(src_np, M))
+
+
+# -------------------------------------------------------- parameter surface
+
+@pytest.mark.parametrize("mode", [(1, 0, (10.0, -5.0, 20.0)), (1, 1, (3.5, -2.0, 7.0)), (0, 2, (1.3, 0.8, 1.1))])
+@pytest.mark.parametrize("resize", [0, 1])
+def test_bigimagewarp_rigid_and_scaling(ctx, mode, resize):
+    wm, dm, para = mode
+    img = vol((40, 50, 60), np.uint8, 2)
+    newsize = (70, 55, 45)
+    out = tw.bigimagewarp(ctx, img, warp_mode=wm, deformation_mode=dm, para=para, resize_mode=resize,
+                          newsize=newsize)
+    osz = newsize if resize else (60, 50, 40)
+    M = tw.make_affine(wm, dm, para, (60, 50, 40), osz)
+    ref = O.affine_warp(img, M, (osz[2], osz[1], osz[0]))
+    agree(out, ref)
+
+
+def test_bigimagewarp_tps_and_affine_modes(ctx):
+    case = synth.plain_tps_case(device="cpu", shape_zyx=(40, 64, 80), n=20, g=4)
+    img = case.vol.numpy()
+    out = tw.bigimagewarp(ctx, img, case.marker_sub, case.marker_tar, warp_mode=0, deformation_mode=1)
+    ref = O.imgwarp_smallmemory_image(case.marker_sub, case.marker_tar, 4, img)
+    agree(out, ref)
+    out_a = tw.bigimagewarp(ctx, img, case.marker_sub, case.marker_tar, warp_mode=0, deformation_mode=0)
+    ref_a = O.affine_warp(img, O.affine_fit(case.marker_tar, case.marker_sub))
+    agree(out_a, ref_a)
+    with pytest.raises(tw.TeraWarpError):
+        tw.bigimagewarp(ctx, img, case.marker_sub, case.marker_tar, device_mode=0)
+
+
+def test_downsample_image(ctx):
+    img = vol((300, 200, 950), np.uint8, 8)
+    out = tw.downsample_image(ctx, img)
+    assert out.shape == (150, 100, 475)
+    M = np.diag([2.0, 2.0, 2.0, 1.0])
+    agree(out, O.affine_warp(img, M, (150, 100, 475)))
