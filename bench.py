@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--small", action="store_true", help="256x256x128 case (for profiling captures)")
+    ap.add_argument("--small", action="store_true", help="256x256x128 case, 64 landmarks")
+    ap.add_argument("--shape", type=str, default="", help="X,Y,Z volume for profiling captures (default: full)")
     return ap.parse_args()
 
 
@@ -209,6 +210,9 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
     shape = (128, 256, 256) if args.small else SHAPE_ZYX
+    if args.shape:
+        sx, sy, sz = (int(v) for v in args.shape.split(","))
+        shape = (sz, sy, sx)
     Z, Y, X = shape
     n = 64 if args.small else N_LANDMARKS
     case = synth.large_tps_case(SEED + rank, dev, shape_zyx=shape, n=n, g=G)
@@ -276,7 +280,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16",
         "data": "synthetic: seeded blob+fibre uint16 volume, jittered-lattice landmarks with sinusoidal displacement",
-        "config": {"workload": WORKLOAD if not args.small else "small_tps_256x256x128_u16_n64_g16",
+        "config": {"workload": (WORKLOAD if not (args.small or args.shape)
+                                else f"tps_{X}x{Y}x{Z}_u16_n{n}_g{G}"),
                    "volume_xyz": [X, Y, Z], "landmarks": n, "grid_spacing": G, "interp": "trilinear",
                    "parallelism": f"replicas x{ws}", "l2": "input 8 GiB > 126 MB L2 (no flush needed)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -311,7 +316,7 @@ def run_ours(args):
         equal = bool(torch.equal(h_dst, dst.cpu()))
         line["e2e"]["matches_device_path"] = equal
         del h_src, h_dst
-    if rank == 0 and ws == 1 and not args.no_cpu and not args.small:
+    if rank == 0 and ws == 1 and not args.no_cpu and not args.small and not args.shape:
         from oracle import oracle as O
         slab_planes = 8
         slab = src[:slab_planes].cpu().numpy()

@@ -186,6 +186,24 @@ typedef int (*tw_read_box_fn)(void *user, int64_t x0, int64_t y0, int64_t z0,
 typedef int (*tw_write_box_fn)(void *user, int64_t x0, int64_t y0, int64_t z0,
                                int64_t nx, int64_t ny, int64_t nz, const void *src);
 
+/* An in-memory volume (x fastest) served by the two functions below.  When
+ * `data` is pinned host memory (cudaHostAlloc / cudaHostRegister), the tiled
+ * entry points recognise these functions and move boxes with strided DMA
+ * copies instead of calling them.  threads: host threads for the copy
+ * (0 = half the cores). */
+typedef struct {
+    void *data;
+    int64_t sz[3];
+    int dtype;
+    int threads;
+} tw_host_volume;
+/* tw_read_box_fn over a tw_host_volume (user = tw_host_volume*). */
+int tw_box_reader_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                       void *dst);
+/* tw_write_box_fn over a tw_host_volume (user = tw_host_volume*). */
+int tw_box_writer_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                       const void *src);
+
 typedef struct {
     int64_t tile[3];        /* output tile dims (0 = 512^3; reference: 1000^3)  */
     int staging_depth;      /* tiles in flight, 2..4 (0 = 2: double buffering)  */

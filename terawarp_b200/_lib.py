@@ -20,6 +20,10 @@ class tw_marker(C.Structure):
     _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
 
 
+class tw_host_volume(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("sz", C.c_int64 * 3), ("dtype", C.c_int), ("threads", C.c_int)]
+
+
 class tw_tile_opts(C.Structure):
     _fields_ = [("tile", C.c_int64 * 3), ("staging_depth", C.c_int), ("interp", C.c_int)]
 
@@ -79,6 +83,8 @@ SIGNATURES = {
                                                READ_BOX, _P, WRITE_BOX, _P, C.POINTER(tw_tile_opts)]),
     "tw_warp_affine_tiled": (C.c_int, [_P, _DP, C.c_int, _I64P, _I64P, READ_BOX, _P, WRITE_BOX, _P,
                                        C.POINTER(tw_tile_opts)]),
+    "tw_box_reader_host": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
+    "tw_box_writer_host": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
     "tw_params_default": (None, [C.POINTER(tw_params)]),
     "tw_output_size": (C.c_int, [C.POINTER(tw_params), _I64P, _I64P]),
     "tw_bigimagewarp": (C.c_int, [_P, C.POINTER(tw_params), _MP, _MP, C.c_int, C.c_int, _P, _I64P, _P]),

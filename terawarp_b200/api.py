@@ -255,6 +255,106 @@ def q_imagewarp_affine_image(ctx: Context, ql_marker_tar, ql_marker_sub, p_img_s
     return out
 
 
+def _tile_opts(tile, depth, interp) -> L.tw_tile_opts:
+    o = L.tw_tile_opts()
+    for a in range(3):
+        o.tile[a] = int(tile[a]) if tile is not None else 0
+    o.staging_depth = int(depth)
+    o.interp = int(interp)
+    return o
+
+
+def _host_volume(x) -> L.tw_host_volume:
+    if _is_torch(x) and x.is_cuda:
+        raise ValueError("tiled paths stream host volumes; pass a host array")
+    v = L.tw_host_volume()
+    v.data = _ptr(x)
+    s = _sz3(x)
+    for a in range(3):
+        v.sz[a] = s[a]
+    v.dtype = _dtype_code(x)
+    v.threads = 0
+    return v
+
+
+def _box_io(src, dst, read_fn=None, write_fn=None):
+    """Tile source / sink: the library's built-in host-volume reader and writer
+    (strided DMA when the array is pinned), or Python callables
+    read_fn(x0, y0, z0, nx, ny, nz) -> array(nz, ny, nx) and
+    write_fn(x0, y0, z0, block) for testing the callback path."""
+    lib = L.load()
+    keep = []
+    if read_fn is None:
+        hv_in = _host_volume(src)
+        keep.append(hv_in)
+        rd = L.READ_BOX(C.cast(lib.tw_box_reader_host, C.c_void_p).value)
+        ru = C.cast(C.pointer(hv_in), C.c_void_p)
+    else:
+        es = 1 if _dtype_code(src) == L.TW_U8 else 2
+
+        def _rd(user, x0, y0, z0, nx, ny, nz, dstp):
+            try:
+                blk = np.ascontiguousarray(read_fn(x0, y0, z0, nx, ny, nz))
+                C.memmove(dstp, blk.ctypes.data, nx * ny * nz * es)
+                return 0
+            except Exception:
+                return 1
+        rd = L.READ_BOX(_rd)
+        ru = None
+    if write_fn is None:
+        hv_out = _host_volume(dst)
+        keep.append(hv_out)
+        wr = L.WRITE_BOX(C.cast(lib.tw_box_writer_host, C.c_void_p).value)
+        wu = C.cast(C.pointer(hv_out), C.c_void_p)
+    else:
+        dt = np.uint8 if _dtype_code(src) == L.TW_U8 else np.uint16
+
+        def _wr(user, x0, y0, z0, nx, ny, nz, srcp):
+            try:
+                buf = (C.c_char * (nx * ny * nz * np.dtype(dt).itemsize)).from_address(srcp)
+                write_fn(x0, y0, z0, np.frombuffer(buf, dtype=dt).reshape(nz, ny, nx).copy())
+                return 0
+            except Exception:
+                return 1
+        wr = L.WRITE_BOX(_wr)
+        wu = None
+    keep += [rd, wr]
+    return rd, ru, wr, wu, keep
+
+
+def imgwarp_smallmemory_tiled(ctx: Context, ql_marker_tar, ql_marker_sub, marker_scale: float, g: int, src, out=None,
+                              tile=(512, 512, 512), depth: int = 2, interp: int = 0, read_fn=None, write_fn=None):
+    """Mirror of imgwarp_smallmemory_CYF for volumes streamed tile by tile
+    (the source may exceed HBM): centres = ql_marker_sub, values =
+    ql_marker_tar, both scaled by marker_scale."""
+    if out is None and write_fn is None:
+        out = _like(src, tuple(src.shape))
+    n = len(np.asarray(ql_marker_tar).reshape(-1, 3))
+    rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
+    opts = _tile_opts(tile, depth, interp)
+    _check(ctx.lib.tw_imgwarp_smallmemory_tiled(ctx.handle, _markers(ql_marker_tar), _markers(ql_marker_sub), n,
+                                                marker_scale, g, _dtype_code(src), _sz3(src), rd, ru, wr, wu,
+                                                C.byref(opts)), ctx, "tw_imgwarp_smallmemory_tiled")
+    del keep
+    return out
+
+
+def warp_affine_tiled(ctx: Context, M, src, out_shape_zyx=None, out=None, tile=(512, 512, 512), depth: int = 2,
+                      interp: int = 0, read_fn=None, write_fn=None):
+    """Affine warp streamed tile by tile (q_imagewarp_affine_cyf)."""
+    shape = tuple(out_shape_zyx) if out_shape_zyx is not None else tuple(src.shape)
+    if out is None and write_fn is None:
+        out = _like(src, shape)
+    Mx = np.ascontiguousarray(np.asarray(M, np.float64).reshape(16))
+    rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
+    opts = _tile_opts(tile, depth, interp)
+    osz = (C.c_int64 * 3)(shape[2], shape[1], shape[0])
+    _check(ctx.lib.tw_warp_affine_tiled(ctx.handle, Mx.ctypes.data_as(L._DP), _dtype_code(src), _sz3(src), osz, rd,
+                                        ru, wr, wu, C.byref(opts)), ctx, "tw_warp_affine_tiled")
+    del keep
+    return out
+
+
 def params(warp_mode=0, device_mode=1, resize_mode=0, deformation_mode=1, para=(1.0, 1.0, 1.0), newsize=(0, 0, 0),
            grid_spacing=4, marker_scale=1.0, lam=0.2, interp=0) -> L.tw_params:
     p = L.tw_params()

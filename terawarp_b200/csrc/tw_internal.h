@@ -53,6 +53,7 @@ struct RJob {
     int64_t bricks[3];     // brick counts along x, y, z
     int64_t brick_begin;   // first flattened brick index of this job in its launch
     int g;                 // grid spacing (TPS)
+    int zs;                // output planes per TPS brick (divides g; set by run_jobs)
     int dtype;             // 1 u8, 2 u16
     int kind;              // 0 affine, 1 TPS
     int interp;            // 0 trilinear, 1 nearest

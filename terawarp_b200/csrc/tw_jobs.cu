@@ -67,12 +67,25 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
 {
     if (njobs <= 0) return TW_OK;
     int64_t total = 0;
-    for (int i = 0; i < njobs; ++i) {
-        int64_t bd[3];
-        brick_dims(jobs[i].kind, jobs[i].g, bd);
-        for (int a = 0; a < 3; ++a) jobs[i].bricks[a] = (jobs[i].out_n[a] + bd[a] - 1) / bd[a];
-        jobs[i].brick_begin = total;
-        total += jobs[i].bricks[0] * jobs[i].bricks[1] * jobs[i].bricks[2];
+    auto count = [&](int zs) {
+        total = 0;
+        for (int i = 0; i < njobs; ++i) {
+            int64_t bd[3];
+            brick_dims(jobs[i].kind, jobs[i].g, bd);
+            if (jobs[i].kind == 1) bd[2] = zs;
+            jobs[i].zs = zs;
+            for (int a = 0; a < 3; ++a) jobs[i].bricks[a] = (jobs[i].out_n[a] + bd[a] - 1) / bd[a];
+            jobs[i].brick_begin = total;
+            total += jobs[i].bricks[0] * jobs[i].bricks[1] * jobs[i].bricks[2];
+        }
+    };
+    // TPS bricks cover one cell layer; when a launch has too few of them to
+    // fill every SM a few times, split each layer over several CTAs
+    int zs = jobs[0].kind == 1 ? jobs[0].g : 8;
+    count(zs);
+    while (jobs[0].kind == 1 && zs > 1 && total < 4 * (int64_t)ctx->sm_count) {
+        zs /= 2;
+        count(zs);
     }
     if (total == 0) return TW_OK;
     RJob *d_jobs = nullptr;

@@ -1,0 +1,392 @@
+// tw_tiled.cpp -- out-of-core tiled warps: the output volume is cut into
+// tiles; each tile's source box (the exact footprint of its samples) is read
+// by a tile source, streamed host -> HBM, warped, and streamed back to a tile
+// sink, with reads, H2D copies, kernels and D2H copies of consecutive tiles
+// overlapped on three streams through a ring of pinned and device slots.
+//
+// Reference: imgwarp_smallmemory_CYF (q_imgwarp_tps_quicksmallmemory.cpp:
+// 1161-1994) and q_imagewarp_affine_cyf (q_warp_affine_tps.cpp:851-1329) loop
+// over 1000^3 tiles synchronously (read, warp, save), estimate each tile's
+// source box from 14 (TPS) or 8 (affine) probe points plus a 60 / 10 voxel
+// halo, and write 0 where a sample falls outside that box.  Here the box is
+// the convex-hull bound of the B-spline over the tile's nodes (or the affine
+// image of the tile's corners), so the tiled output equals the whole-volume
+// output voxel for voxel.
+#include "tw_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+using namespace tw;
+
+namespace {
+
+size_t esize(int dtype) { return dtype == TW_U8 ? 1 : 2; }
+
+struct Box {
+    int64_t o[3];   // origin
+    int64_t n[3];   // extent (0 on any axis = empty)
+    int64_t count() const { return n[0] * n[1] * n[2]; }
+};
+
+struct TileIO {
+    tw_read_box_fn read;
+    void *read_user;
+    tw_write_box_fn write;
+    void *write_user;
+};
+
+struct Slot {
+    void *d_src = nullptr, *d_dst = nullptr;
+    void *h_src = nullptr, *h_dst = nullptr;
+    cudaEvent_t e_in = nullptr, e_comp = nullptr, e_out = nullptr;
+    int64_t tile = -1;       // tile whose result is in flight in this slot
+};
+
+// Source-box bound for a tile from the hull of its sample positions.
+Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3])
+{
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+        if (!std::isfinite(lo[a]) || !std::isfinite(hi[a])) {  // degenerate field: read everything
+            b.o[a] = 0;
+            b.n[a] = sz[a];
+            continue;
+        }
+        int64_t l = (int64_t)std::floor((double)lo[a]) - 1;
+        int64_t h = (int64_t)std::floor((double)hi[a]) + 2;
+        l = std::max<int64_t>(l, 0);
+        h = std::min<int64_t>(h, sz[a] - 1);
+        b.o[a] = l;
+        b.n[a] = h >= l ? h - l + 1 : 0;
+    }
+    return b;
+}
+
+// Copies a box between a host volume and a device buffer with the DMA
+// engine (strided 3-D copy, no host CPU work).
+cudaError_t copy_box(void *dst, const void *src, int64_t dst_x, int64_t dst_y, const int64_t dst_off[3],
+                     int64_t src_x, int64_t src_y, const int64_t src_off[3], const int64_t n[3], size_t es,
+                     cudaMemcpyKind kind, cudaStream_t st)
+{
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    p.srcPtr = make_cudaPitchedPtr(const_cast<void *>(src), (size_t)src_x * es, (size_t)src_x, (size_t)src_y);
+    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)dst_x * es, (size_t)dst_x, (size_t)dst_y);
+    p.srcPos = make_cudaPos((size_t)src_off[0] * es, (size_t)src_off[1], (size_t)src_off[2]);
+    p.dstPos = make_cudaPos((size_t)dst_off[0] * es, (size_t)dst_off[1], (size_t)dst_off[2]);
+    p.extent = make_cudaExtent((size_t)n[0] * es, (size_t)n[1], (size_t)n[2]);
+    p.kind = kind;
+    return cudaMemcpy3DAsync(&p, st);
+}
+
+tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const double *M, int dtype, int interp,
+                    const int64_t src_sz[3], const int64_t out_sz[3], const TileIO &io, const tw_tile_opts *opts)
+{
+    const size_t es = esize(dtype);
+    int64_t T[3] = {512, 512, 512};
+    int depth = 2;
+    if (opts) {
+        for (int a = 0; a < 3; ++a)
+            if (opts->tile[a] > 0) T[a] = opts->tile[a];
+        if (opts->staging_depth > 0) depth = std::min(4, std::max(2, opts->staging_depth));
+    }
+    if (kind == 1)  // TPS tiles start on control-cell boundaries
+        for (int a = 0; a < 3; ++a) T[a] = std::max<int64_t>(g, (T[a] / g) * g);
+    for (int a = 0; a < 3; ++a) T[a] = std::min(T[a], out_sz[a]);
+    int64_t nt[3];
+    for (int a = 0; a < 3; ++a) nt[a] = (out_sz[a] + T[a] - 1) / T[a];
+    const int64_t ntiles = nt[0] * nt[1] * nt[2];
+
+    // tile boxes and their source footprints
+    std::vector<Box> tiles(ntiles), srcs(ntiles);
+    for (int64_t t = 0; t < ntiles; ++t) {
+        int64_t ix = t % nt[0], iy = (t / nt[0]) % nt[1], iz = t / (nt[0] * nt[1]);
+        const int64_t idx[3] = {ix, iy, iz};
+        for (int a = 0; a < 3; ++a) {
+            tiles[t].o[a] = idx[a] * T[a];
+            tiles[t].n[a] = std::min(T[a], out_sz[a] - tiles[t].o[a]);
+        }
+    }
+    if (kind == 1) {
+        std::vector<CellBox> cb(ntiles);
+        for (int64_t t = 0; t < ntiles; ++t)
+            for (int a = 0; a < 3; ++a) {
+                cb[t].c0[a] = tiles[t].o[a] / g;
+                cb[t].c1[a] = (tiles[t].o[a] + tiles[t].n[a] + g - 1) / g;
+            }
+        const int64_t gsz[3] = {grid_size(out_sz[0], g), grid_size(out_sz[1], g), grid_size(out_sz[2], g)};
+        std::vector<float> lo, hi;
+        TW_TRY(tps_box_hull(ctx, nodes, gsz, g, cb, ctx->stream, lo, hi));
+        for (int64_t t = 0; t < ntiles; ++t) srcs[t] = box_from_hull(&lo[3 * t], &hi[3 * t], src_sz);
+    } else {
+        for (int64_t t = 0; t < ntiles; ++t) {
+            float lo[3], hi[3];
+            for (int r = 0; r < 3; ++r) {
+                double mn = 1e300, mxv = -1e300;
+                for (int c = 0; c < 8; ++c) {
+                    double p[3];
+                    for (int a = 0; a < 3; ++a)
+                        p[a] = (double)tiles[t].o[a] + (((c >> a) & 1) ? (double)(tiles[t].n[a] - 1) : 0.0);
+                    double q = M[r * 4] * p[0] + M[r * 4 + 1] * p[1] + M[r * 4 + 2] * p[2] + M[r * 4 + 3];
+                    mn = std::min(mn, q);
+                    mxv = std::max(mxv, q);
+                }
+                lo[r] = (float)mn;
+                hi[r] = (float)mxv;
+            }
+            srcs[t] = box_from_hull(lo, hi, src_sz);
+        }
+    }
+    int64_t max_src = 1, max_out = 1;
+    for (int64_t t = 0; t < ntiles; ++t) {
+        max_src = std::max(max_src, srcs[t].count());
+        max_out = std::max(max_out, tiles[t].count());
+    }
+
+    // the built-in host-volume reader/writer on pinned memory become DMA copies
+    const tw_host_volume *hv_in = io.read == tw_box_reader_host ? static_cast<const tw_host_volume *>(io.read_user)
+                                                                  : nullptr;
+    const tw_host_volume *hv_out = io.write == tw_box_writer_host ? static_cast<const tw_host_volume *>(io.write_user)
+                                                                    : nullptr;
+    const bool dma_in = hv_in && is_pinned_ptr(hv_in->data);
+    const bool dma_out = hv_out && is_pinned_ptr(hv_out->data);
+    for (int a = 0; a < 3; ++a) {
+        if (hv_in && (hv_in->sz[a] != src_sz[a] || hv_in->dtype != dtype))
+            return fail(ctx, TW_ERR_ARG, "tile source volume does not match the source dims / dtype");
+        if (hv_out && (hv_out->sz[a] != out_sz[a] || hv_out->dtype != dtype))
+            return fail(ctx, TW_ERR_ARG, "tile sink volume does not match the output dims / dtype");
+    }
+
+    std::vector<Slot> slots(depth);
+    struct Cleanup {
+        tw_ctx *ctx;
+        std::vector<Slot> &s;
+        size_t sb, ob;
+        ~Cleanup()
+        {
+            for (auto &x : s) {
+                if (x.d_src) dfree(ctx, x.d_src, sb);
+                if (x.d_dst) dfree(ctx, x.d_dst, ob);
+                if (x.h_src) cudaFreeHost(x.h_src);
+                if (x.h_dst) cudaFreeHost(x.h_dst);
+                if (x.e_in) cudaEventDestroy(x.e_in);
+                if (x.e_comp) cudaEventDestroy(x.e_comp);
+                if (x.e_out) cudaEventDestroy(x.e_out);
+            }
+        }
+    } cleanup{ctx, slots, (size_t)max_src * es, (size_t)max_out * es};
+    for (auto &s : slots) {
+        TW_TRY(dmalloc(ctx, &s.d_src, (size_t)max_src * es));
+        TW_TRY(dmalloc(ctx, &s.d_dst, (size_t)max_out * es));
+        if (!dma_in) TW_CUDA_TRY(cudaHostAlloc(&s.h_src, (size_t)max_src * es, cudaHostAllocDefault));
+        if (!dma_out) TW_CUDA_TRY(cudaHostAlloc(&s.h_dst, (size_t)max_out * es, cudaHostAllocDefault));
+        TW_CUDA_TRY(cudaEventCreateWithFlags(&s.e_in, cudaEventDisableTiming));
+        TW_CUDA_TRY(cudaEventCreateWithFlags(&s.e_comp, cudaEventDisableTiming));
+        TW_CUDA_TRY(cudaEventCreateWithFlags(&s.e_out, cudaEventDisableTiming));
+    }
+
+    // hands a finished tile to the sink (after its D2H completed)
+    auto retire = [&](Slot &s) -> tw_status {
+        if (s.tile < 0) return TW_OK;
+        TW_CUDA_TRY(cudaEventSynchronize(s.e_out));
+        const Box &b = tiles[s.tile];
+        if (!dma_out && io.write) {
+            if (io.write(io.write_user, b.o[0], b.o[1], b.o[2], b.n[0], b.n[1], b.n[2], s.h_dst) != 0)
+                return fail(ctx, TW_ERR_IO, "tile sink failed at tile " + std::to_string(s.tile));
+        }
+        s.tile = -1;
+        return TW_OK;
+    };
+
+    for (int64_t t = 0; t < ntiles; ++t) {
+        Slot &s = slots[t % depth];
+        TW_TRY(retire(s));  // frees the slot's pinned output and, transitively, its device buffers
+        const Box &tb = tiles[t];
+        const Box &sb = srcs[t];
+        const bool empty = sb.count() == 0;
+        // 1. source box -> device slot
+        if (!empty) {
+            const int64_t zero[3] = {0, 0, 0};
+            if (dma_in) {
+                TW_CUDA_TRY(copy_box(s.d_src, hv_in->data, sb.n[0], sb.n[1], zero, hv_in->sz[0], hv_in->sz[1], sb.o,
+                                     sb.n, es, cudaMemcpyHostToDevice, ctx->h2d));
+            } else {
+                if (!io.read) return fail(ctx, TW_ERR_ARG, "no tile source");
+                if (io.read(io.read_user, sb.o[0], sb.o[1], sb.o[2], sb.n[0], sb.n[1], sb.n[2], s.h_src) != 0)
+                    return fail(ctx, TW_ERR_IO, "tile source failed at tile " + std::to_string(t));
+                TW_CUDA_TRY(cudaMemcpyAsync(s.d_src, s.h_src, (size_t)sb.count() * es, cudaMemcpyHostToDevice,
+                                            ctx->h2d));
+            }
+        }
+        TW_CUDA_TRY(cudaEventRecord(s.e_in, ctx->h2d));
+        // 2. warp the tile (or zero it when no sample can land in the volume)
+        TW_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, s.e_in, 0));
+        if (empty) {
+            TW_CUDA_TRY(cudaMemsetAsync(s.d_dst, 0, (size_t)tb.count() * es, ctx->stream));
+        } else {
+            RJob j;
+            if (kind == 1) {
+                j = tps_job(s.d_src, src_sz, s.d_dst, out_sz, nodes, g, dtype, interp);
+            } else {
+                j = affine_job(s.d_src, src_sz, s.d_dst, out_sz, M, dtype, interp);
+            }
+            for (int a = 0; a < 3; ++a) {
+                j.src_o[a] = sb.o[a];
+                j.src_n[a] = sb.n[a];
+                j.out_o[a] = tb.o[a];
+                j.out_n[a] = tb.n[a];
+            }
+            j.src_py = sb.n[0];
+            j.src_pz = sb.n[0] * sb.n[1];
+            j.dst_py = tb.n[0];
+            j.dst_pz = tb.n[0] * tb.n[1];
+            TW_TRY(run_jobs(ctx, &j, 1, ctx->stream));
+        }
+        TW_CUDA_TRY(cudaEventRecord(s.e_comp, ctx->stream));
+        // 3. tile -> host (retire() has already waited for this slot's
+        // previous tile, so its buffers are free for the next use)
+        TW_CUDA_TRY(cudaStreamWaitEvent(ctx->d2h, s.e_comp, 0));
+        const int64_t zero[3] = {0, 0, 0};
+        if (dma_out) {
+            TW_CUDA_TRY(copy_box(hv_out->data, s.d_dst, hv_out->sz[0], hv_out->sz[1], tb.o, tb.n[0], tb.n[1], zero,
+                                 tb.n, es, cudaMemcpyDeviceToHost, ctx->d2h));
+        } else {
+            TW_CUDA_TRY(cudaMemcpyAsync(s.h_dst, s.d_dst, (size_t)tb.count() * es, cudaMemcpyDeviceToHost, ctx->d2h));
+        }
+        TW_CUDA_TRY(cudaEventRecord(s.e_out, ctx->d2h));
+        s.tile = t;
+    }
+    for (int64_t t = std::max<int64_t>(0, ntiles - depth); t < ntiles; ++t) TW_TRY(retire(slots[t % depth]));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->h2d));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->d2h));
+    return TW_OK;
+}
+
+void copy_rows(char *dst, const char *src, int64_t nrows, size_t row_bytes, int64_t dst_pitch, int64_t src_pitch,
+               int threads)
+{
+    auto work = [&](int64_t r0, int64_t r1) {
+        for (int64_t r = r0; r < r1; ++r) std::memcpy(dst + r * dst_pitch, src + r * src_pitch, row_bytes);
+    };
+    if (threads <= 1 || nrows < 64) {
+        work(0, nrows);
+        return;
+    }
+    std::vector<std::thread> th;
+    const int64_t per = (nrows + threads - 1) / threads;
+    for (int i = 0; i < threads; ++i) {
+        const int64_t r0 = i * per, r1 = std::min(nrows, r0 + per);
+        if (r0 < r1) th.emplace_back(work, r0, r1);
+    }
+    for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+int tw_box_reader_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz, void *dst)
+{
+    const tw_host_volume *v = static_cast<const tw_host_volume *>(user);
+    if (!v || !v->data || !dst) return 1;
+    const size_t es = esize(v->dtype);
+    if (x0 < 0 || y0 < 0 || z0 < 0 || x0 + nx > v->sz[0] || y0 + ny > v->sz[1] || z0 + nz > v->sz[2]) return 2;
+    // row r of the box = (y, z) = (r % ny, r / ny)
+    const int threads = v->threads > 0 ? v->threads : (int)std::max(1u, std::thread::hardware_concurrency() / 2);
+    auto work = [&](int64_t r0, int64_t r1) {
+        for (int64_t r = r0; r < r1; ++r) {
+            const int64_t y = r % ny, z = r / ny;
+            std::memcpy(static_cast<char *>(dst) + (size_t)r * nx * es,
+                        static_cast<const char *>(v->data) + (((z0 + z) * v->sz[1] + (y0 + y)) * v->sz[0] + x0) * es,
+                        (size_t)nx * es);
+        }
+    };
+    const int64_t rows = ny * nz;
+    if (threads <= 1 || rows < 64) {
+        work(0, rows);
+        return 0;
+    }
+    std::vector<std::thread> th;
+    const int64_t per = (rows + threads - 1) / threads;
+    for (int i = 0; i < threads; ++i) {
+        const int64_t r0 = i * per, r1 = std::min(rows, r0 + per);
+        if (r0 < r1) th.emplace_back(work, r0, r1);
+    }
+    for (auto &x : th) x.join();
+    return 0;
+}
+
+int tw_box_writer_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                       const void *src)
+{
+    const tw_host_volume *v = static_cast<const tw_host_volume *>(user);
+    if (!v || !v->data || !src) return 1;
+    const size_t es = esize(v->dtype);
+    if (x0 < 0 || y0 < 0 || z0 < 0 || x0 + nx > v->sz[0] || y0 + ny > v->sz[1] || z0 + nz > v->sz[2]) return 2;
+    const int threads = v->threads > 0 ? v->threads : (int)std::max(1u, std::thread::hardware_concurrency() / 2);
+    for (int64_t z = 0; z < nz; ++z)
+        copy_rows(static_cast<char *>(v->data) + (((z0 + z) * v->sz[1] + y0) * v->sz[0] + x0) * es,
+                  static_cast<const char *>(src) + (size_t)z * nx * ny * es, ny, (size_t)nx * es,
+                  (int64_t)(v->sz[0] * es), (int64_t)(nx * es), nz > 1 ? 1 : threads);
+    return 0;
+}
+
+tw_status tw_imgwarp_smallmemory_tiled(tw_ctx *ctx, const tw_marker *ql_marker_tar, const tw_marker *ql_marker_sub,
+                                       int n, double marker_scale, int g, int dtype, const int64_t sz[3],
+                                       tw_read_box_fn read_box, void *read_user, tw_write_box_fn write_box,
+                                       void *write_user, const tw_tile_opts *opts)
+{
+    if (!ctx || !sz) return TW_ERR_ARG;
+    if (!ql_marker_tar || !ql_marker_sub || n <= 0) return fail(ctx, TW_ERR_ARG, "target or subject control points is invalid");
+    if (!g_supported(g)) return fail(ctx, TW_ERR_UNSUPPORTED, "grid spacing must be 4, 8, 16, 32 or 64");
+    if (dtype != TW_U8 && dtype != TW_U16) return fail(ctx, TW_ERR_ARG, "dtype must be TW_U8 or TW_U16");
+    for (int a = 0; a < 3; ++a)
+        if (sz[a] < 1) return fail(ctx, TW_ERR_ARG, "volume size is invalid");
+    if (!read_box || !write_box) return fail(ctx, TW_ERR_ARG, "tile source and sink are required");
+    const int interp = opts ? opts->interp : 0;
+    if (interp != 0 && interp != 1) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    const double scale = marker_scale > 0 ? marker_scale : 1.0;
+    tw_tps *tp = nullptr;
+    // the reference solves once per job with the markers scaled by 4
+    // (q_imgwarp_tps_quicksmallmemory.cpp:1194-1203, :1212)
+    TW_TRY(make_tps(ctx, ql_marker_sub, ql_marker_tar, n, 0.2, scale, ctx->stream, &tp));
+    std::unique_ptr<tw_tps, void (*)(tw_tps *)> guard(tp, destroy_tps);
+    const int64_t gsz[3] = {grid_size(sz[0], g), grid_size(sz[1], g), grid_size(sz[2], g)};
+    void *nodes = nullptr;
+    const size_t nbytes = sizeof(float4) * (size_t)(gsz[0] * gsz[1] * gsz[2]);
+    TW_TRY(dmalloc(ctx, &nodes, nbytes));
+    const int64_t off[3] = {0, 0, 0};
+    tw_status s = eval_grid(ctx, tp, gsz, g, off, static_cast<float4 *>(nodes), ctx->stream);
+    if (s == TW_OK) {
+        TileIO io{read_box, read_user, write_box, write_user};
+        s = run_tiled(ctx, 1, static_cast<const float4 *>(nodes), g, nullptr, dtype, interp, sz, sz, io, opts);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, nodes, nbytes);
+    return s;
+}
+
+tw_status tw_warp_affine_tiled(tw_ctx *ctx, const double M[16], int dtype, const int64_t src_sz[3],
+                               const int64_t out_sz[3], tw_read_box_fn read_box, void *read_user,
+                               tw_write_box_fn write_box, void *write_user, const tw_tile_opts *opts)
+{
+    if (!ctx || !M || !src_sz || !out_sz) return TW_ERR_ARG;
+    if (dtype != TW_U8 && dtype != TW_U16) return fail(ctx, TW_ERR_ARG, "dtype must be TW_U8 or TW_U16");
+    for (int a = 0; a < 3; ++a)
+        if (src_sz[a] < 1 || out_sz[a] < 1) return fail(ctx, TW_ERR_ARG, "volume size is invalid");
+    if (!read_box || !write_box) return fail(ctx, TW_ERR_ARG, "tile source and sink are required");
+    const int interp = opts ? opts->interp : 0;
+    if (interp != 0 && interp != 1) return TW_ERR_ARG;
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    TileIO io{read_box, read_user, write_box, write_user};
+    return run_tiled(ctx, 0, nullptr, 0, M, dtype, interp, src_sz, out_sz, io, opts);
+}
+
+}  // extern "C"

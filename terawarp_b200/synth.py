@@ -85,6 +85,7 @@ def jitter_landmarks(sz_xyz, n: int, seed: int, margin: float = 16.0, sigma: flo
     """Subject points uniform in the interior; target = subject + N(0, sigma)
     per axis.  Returns (subject, target) as (n, 3) float32 x, y, z."""
     rng = np.random.default_rng(seed)
+    margin = min(margin, min(sz_xyz) / 4.0)
     lo = np.array([margin] * 3)
     hi = np.array(sz_xyz, dtype=np.float64) - 1 - margin
     sub = rng.uniform(lo, hi, size=(n, 3))
