@@ -355,6 +355,81 @@ def warp_affine_tiled(ctx: Context, M, src, out_shape_zyx=None, out=None, tile=(
     return out
 
 
+class Server:
+    """Continuous-batching warp server (tw_server): jobs are admitted by HBM
+    budget as they arrive, their resample work is batched into persistent
+    launches, and results land in the caller's host buffers."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_inflight: int = 16):
+        self.ctx = ctx
+        h = C.c_void_p()
+        _check(ctx.lib.tw_server_create(ctx.handle, hbm_budget_bytes, max_inflight, C.byref(h)), ctx,
+               "tw_server_create")
+        self.handle = h
+        self._keep = {}
+
+    def _submit(self, job: L.tw_job, keep) -> int:
+        jid = C.c_uint64()
+        _check(self.ctx.lib.tw_server_submit(self.handle, C.byref(job), C.byref(jid)), None, "tw_server_submit")
+        self._keep[jid.value] = keep
+        return jid.value
+
+    def submit_affine(self, M, src, dst, interp: int = 0) -> int:
+        j = L.tw_job()
+        j.kind, j.dtype, j.interp, j.g = 0, _dtype_code(src), interp, 0
+        s, d = _sz3(src), _sz3(dst)
+        for a in range(3):
+            j.src_sz[a], j.dst_sz[a] = s[a], d[a]
+        for i, v in enumerate(np.asarray(M, np.float64).reshape(16)):
+            j.M[i] = float(v)
+        j.src, j.dst = _ptr(src), _ptr(dst)
+        return self._submit(j, (src, dst))
+
+    def submit_tps(self, centres, values, g: int, src, dst, lam: float = 0.2, interp: int = 0) -> int:
+        """centres = target-image landmarks (TPS centres), values = subject-image landmarks."""
+        j = L.tw_job()
+        j.kind, j.dtype, j.interp, j.g = 1, _dtype_code(src), interp, g
+        s, d = _sz3(src), _sz3(dst)
+        for a in range(3):
+            j.src_sz[a], j.dst_sz[a] = s[a], d[a]
+        c, v = _markers(centres), _markers(values)
+        j.centres = C.cast(c, C.POINTER(L.tw_marker))
+        j.values = C.cast(v, C.POINTER(L.tw_marker))
+        j.n = len(np.asarray(centres).reshape(-1, 3))
+        j.lambda_ = lam
+        j.src, j.dst = _ptr(src), _ptr(dst)
+        return self._submit(j, (src, dst, c, v))
+
+    def poll(self, job_id: int):
+        """(done, latency_s); raises on a failed job."""
+        lat = C.c_double()
+        st = self.ctx.lib.tw_server_poll(self.handle, job_id, C.byref(lat))
+        if st == L.TW_ERR_NOT_READY:
+            return False, None
+        self._keep.pop(job_id, None)
+        _check(st, None, f"server job {job_id}")
+        return True, lat.value
+
+    def wait(self, job_id: int, timeout_s: float = 600.0) -> float:
+        lat = C.c_double()
+        st = self.ctx.lib.tw_server_wait(self.handle, job_id, timeout_s, C.byref(lat))
+        self._keep.pop(job_id, None)
+        _check(st, None, f"server job {job_id}")
+        return lat.value
+
+    def close(self) -> None:
+        if self.handle:
+            self.ctx.lib.tw_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 def params(warp_mode=0, device_mode=1, resize_mode=0, deformation_mode=1, para=(1.0, 1.0, 1.0), newsize=(0, 0, 0),
            grid_spacing=4, marker_scale=1.0, lam=0.2, interp=0) -> L.tw_params:
     p = L.tw_params()

@@ -33,20 +33,27 @@ tw_status dmalloc(tw_ctx *ctx, void **p, size_t bytes)
         ctx->used.fetch_sub(bytes);
         return fail(ctx, TW_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget");
     }
-    cudaError_t e = cudaMalloc(p, bytes);
+    // stream-ordered allocation from the context's pool on its compute
+    // stream, made visible to every stream of the context before returning
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         ctx->used.fetch_sub(bytes);
         *p = nullptr;
         cudaGetLastError();
-        return fail(ctx, TW_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        return fail(ctx, TW_ERR_OOM, std::string("device allocation: ") + cudaGetErrorString(e));
     }
     return TW_OK;
 }
 
+// Returns a block to the pool once all work queued so far on the context's
+// streams is done (callers free only after their last use was enqueued).
 void dfree(tw_ctx *ctx, void *p, size_t bytes)
 {
     if (!p) return;
-    cudaFree(p);
+    cudaStreamSynchronize(ctx->h2d);
+    cudaStreamSynchronize(ctx->d2h);
+    cudaFreeAsync(p, ctx->stream);
     ctx->used.fetch_sub(bytes);
 }
 
@@ -213,6 +220,17 @@ tw_status tw_ctx_create(int device, size_t hbm_budget_bytes, tw_ctx **out)
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return TW_ERR_CUDA;
     if (cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking) != cudaSuccess) return TW_ERR_CUDA;
     if (cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking) != cudaSuccess) return TW_ERR_CUDA;
+    // a private pool (not the device's default pool) that caches freed blocks
+    // for the context's lifetime, so per-call workspaces cost no cudaMalloc
+    cudaMemPoolProps pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &pp) != cudaSuccess) return TW_ERR_CUDA;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     *out = c.release();
     return TW_OK;
 }
@@ -227,6 +245,7 @@ tw_status tw_ctx_destroy(tw_ctx *ctx)
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
     if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return TW_OK;
 }

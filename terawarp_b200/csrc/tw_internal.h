@@ -108,6 +108,7 @@ struct tw_ctx {
     cudaStream_t stream = nullptr;      // compute
     cudaStream_t h2d = nullptr;         // host -> device copies
     cudaStream_t d2h = nullptr;         // device -> host copies
+    cudaMemPool_t pool = nullptr;       // stream-ordered pool that keeps freed blocks
     std::atomic<uint64_t> launches{0};
     mutable std::mutex err_mu;
     std::string last_error;

@@ -384,10 +384,14 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
 
     // a brick spans zs output planes of one cell layer (zs divides G; small
     // jobs split the layer over several CTAs to fill the machine)
+    // The frame origin O is the brick's corner with z at the start of its cell
+    // layer, so sample positions (and their FP32 rounding) do not depend on
+    // how a launch splits layers: a job gives the same voxels alone or batched.
     const int zs = J.zs;
-    const int64_t O[3] = {J.out_o[0] + bx * Gm::BX, J.out_o[1] + by * Gm::BY, J.out_o[2] + bz * zs};
+    const int64_t zfirst = J.out_o[2] + bz * zs;          // first output plane of this brick
+    const int64_t O[3] = {J.out_o[0] + bx * Gm::BX, J.out_o[1] + by * Gm::BY, (zfirst / G) * G};
     const int64_t c0[3] = {O[0] / G, O[1] / G, O[2] / G};  // first cell (= first node index)
-    const int zoff = (int)(O[2] - c0[2] * G);              // first plane within the cell layer
+    const int zoff = (int)(zfirst - O[2]);                 // first plane within the cell layer
 
     // 1. stage node' = DF + node position - O, and its hull (a non-finite
     // node forces the checked path)
@@ -419,7 +423,7 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
 
     const bool inside_out = (O[0] + Gm::BX <= J.out_o[0] + J.out_n[0]) &&
                             (O[1] + Gm::BY <= J.out_o[1] + J.out_n[1]) &&
-                            (O[2] + zs <= J.out_o[2] + J.out_n[2]);
+                            (zfirst + zs <= J.out_o[2] + J.out_n[2]);
     const bool fast = inside_out && hull_inside(J, O, mn, mx);
     const Frame frame = make_frame(J, O);
     const bool span_ok = offsets_fit_32(J, mn, mx);
@@ -479,12 +483,13 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     const int64_t sbase = (O[2] - J.src_o[2]) * J.src_pz + (O[1] - J.src_o[1]) * J.src_py + (O[0] - J.src_o[0]);
     const T *base = src + sbase;
     const int py32 = (int)J.src_py, pz32 = (int)J.src_pz;
-    const int64_t dbase0 = (O[2] - J.out_o[2]) * J.dst_pz + (O[1] - J.out_o[1]) * J.dst_py + (O[0] - J.out_o[0]);
+    // output plane z of the loop below is zfirst + z
+    const int64_t dbase0 = (zfirst - J.out_o[2]) * J.dst_pz + (O[1] - J.out_o[1]) * J.dst_py + (O[0] - J.out_o[0]);
     // a voxel pair (even x) can be written as one 2-element store
     const bool pair_ok = ((((uintptr_t)(dst + dbase0)) % (2 * sizeof(T))) == 0) && (J.dst_py % 2 == 0) &&
                          (J.dst_pz % 2 == 0);
     const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
-    const int64_t ze = J.out_o[2] + J.out_n[2] - O[2];
+    const int64_t ze = J.out_o[2] + J.out_n[2] - zfirst;
 
     for (int z = 0; z < zs; ++z) {
         float4 *Q = Qb + (z & 1) * (Gm::BY * Gm::NX);

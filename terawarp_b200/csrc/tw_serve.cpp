@@ -1,0 +1,361 @@
+// tw_serve.cpp -- continuous-batching warp server.
+//
+// Jobs (affine or TPS, uint8 or uint16, any size) are submitted from any
+// thread.  One worker thread owns a private context and loops:
+//   1. admission: FIFO, while the HBM reservation of the next job fits the
+//      budget and fewer than max_inflight jobs are on the device -- its
+//      landmarks are solved (FP64), its node grid evaluated and its source
+//      volume copied to HBM on a stream of its own;
+//   2. batching: every job whose inputs are resident joins the next resample
+//      round; jobs sharing (dtype, kind, g, interp) run in one persistent
+//      launch over all their bricks, so work of jobs that arrived at
+//      different times overlaps on the device;
+//   3. completion: each job's result is copied back on its own stream while
+//      later rounds compute, and its latency (submit -> result in host
+//      memory) is recorded.
+// Every job gives the same voxels alone or batched: the kernels' arithmetic
+// depends only on the job, never on the launch it shares.
+// The reference has no serving mode.
+#include "tw_host.h"
+
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <thread>
+#include <vector>
+
+using namespace tw;
+
+namespace {
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+size_t esize(int dtype) { return dtype == TW_U8 ? 1 : 2; }
+
+enum JobState { kQueued = 0, kPrepared = 1, kComputing = 2, kDone = 3 };
+
+struct JobRec {
+    uint64_t id = 0;
+    tw_job spec;
+    std::vector<tw_marker> ctr, val;
+    double t_submit = 0, t_done = 0;
+    tw_status status = TW_ERR_NOT_READY;
+    int state = kQueued;
+    size_t reserve = 0;
+    void *d_src = nullptr, *d_dst = nullptr, *d_nodes = nullptr;
+    size_t src_b = 0, dst_b = 0, nodes_b = 0;
+    tw_tps *tps = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_done = nullptr;
+};
+
+}  // namespace
+
+struct tw_server {
+    tw_ctx *ctx = nullptr;  // private context of the worker
+    size_t budget = 0, used = 0;
+    int max_inflight = 8;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<JobRec *> queued;
+    std::map<uint64_t, std::unique_ptr<JobRec>> jobs;
+    std::vector<JobRec *> active;
+    std::vector<cudaStream_t> streams;
+    cudaStream_t batch = nullptr;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+};
+
+namespace {
+
+size_t job_reserve(const JobRec &j)
+{
+    const tw_job &s = j.spec;
+    const size_t es = esize(s.dtype);
+    size_t b = es * (size_t)(s.src_sz[0] * s.src_sz[1] * s.src_sz[2]) +
+               es * (size_t)(s.dst_sz[0] * s.dst_sz[1] * s.dst_sz[2]);
+    if (s.kind == 1) {
+        b += sizeof(float4) * (size_t)(grid_size(s.dst_sz[0], s.g) * grid_size(s.dst_sz[1], s.g) *
+                                       grid_size(s.dst_sz[2], s.g));
+        const size_t m = s.n > 4 ? (size_t)(s.n - 4) : 0;
+        b += sizeof(double) * (m * m + 48 * (size_t)s.n + 64);  // solve workspace
+    }
+    return b;
+}
+
+void release(tw_server *s, JobRec *j)
+{
+    if (j->st) {
+        if (j->d_src) cudaFreeAsync(j->d_src, j->st);
+        if (j->d_dst) cudaFreeAsync(j->d_dst, j->st);
+        if (j->d_nodes) cudaFreeAsync(j->d_nodes, j->st);
+    }
+    j->d_src = j->d_dst = j->d_nodes = nullptr;
+    if (j->tps) {
+        destroy_tps(j->tps);
+        j->tps = nullptr;
+    }
+    if (j->ev_ready) cudaEventDestroy(j->ev_ready);
+    if (j->ev_done) cudaEventDestroy(j->ev_done);
+    j->ev_ready = j->ev_done = nullptr;
+    if (j->st) s->streams.push_back(j->st);
+    j->st = nullptr;
+}
+
+// Puts a job's inputs on the device: FP64 solve + node grid (TPS) and the
+// source volume, all on the job's own stream.
+tw_status prepare(tw_server *s, JobRec *j)
+{
+    tw_ctx *ctx = s->ctx;
+    const tw_job &sp = j->spec;
+    const size_t es = esize(sp.dtype);
+    if (s->streams.empty()) {
+        cudaStream_t st;
+        TW_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        s->streams.push_back(st);
+    }
+    j->st = s->streams.back();
+    s->streams.pop_back();
+    TW_CUDA_TRY(cudaEventCreateWithFlags(&j->ev_ready, cudaEventDisableTiming));
+    TW_CUDA_TRY(cudaEventCreateWithFlags(&j->ev_done, cudaEventDisableTiming));
+    if (sp.kind == 1) {
+        // solve first: its host synchronisation then waits for the solve only
+        TW_TRY(make_tps(ctx, j->ctr.data(), j->val.data(), sp.n, sp.lambda > 0 ? sp.lambda : 0.2, 1.0, j->st,
+                        &j->tps));
+        const int64_t gsz[3] = {grid_size(sp.dst_sz[0], sp.g), grid_size(sp.dst_sz[1], sp.g),
+                                grid_size(sp.dst_sz[2], sp.g)};
+        j->nodes_b = sizeof(float4) * (size_t)(gsz[0] * gsz[1] * gsz[2]);
+        TW_CUDA_TRY(cudaMallocFromPoolAsync(&j->d_nodes, j->nodes_b, ctx->pool, j->st));
+        const int64_t off[3] = {0, 0, 0};
+        TW_TRY(eval_grid(ctx, j->tps, gsz, sp.g, off, static_cast<float4 *>(j->d_nodes), j->st));
+    }
+    j->src_b = es * (size_t)(sp.src_sz[0] * sp.src_sz[1] * sp.src_sz[2]);
+    j->dst_b = es * (size_t)(sp.dst_sz[0] * sp.dst_sz[1] * sp.dst_sz[2]);
+    TW_CUDA_TRY(cudaMallocFromPoolAsync(&j->d_src, j->src_b, ctx->pool, j->st));
+    TW_CUDA_TRY(cudaMallocFromPoolAsync(&j->d_dst, j->dst_b, ctx->pool, j->st));
+    TW_CUDA_TRY(cudaMemcpyAsync(j->d_src, sp.src, j->src_b, cudaMemcpyHostToDevice, j->st));
+    TW_CUDA_TRY(cudaEventRecord(j->ev_ready, j->st));
+    return TW_OK;
+}
+
+// One resample round over every prepared job whose inputs are resident.
+tw_status batch_round(tw_server *s, std::vector<JobRec *> &ready)
+{
+    tw_ctx *ctx = s->ctx;
+    std::map<std::tuple<int, int, int, int>, std::vector<JobRec *>> groups;
+    for (JobRec *j : ready) groups[{j->spec.dtype, j->spec.kind, j->spec.g, j->spec.interp}].push_back(j);
+    for (auto &kv : groups) {
+        std::vector<RJob> rj;
+        for (JobRec *j : kv.second) {
+            TW_CUDA_TRY(cudaStreamWaitEvent(s->batch, j->ev_ready, 0));
+            const tw_job &sp = j->spec;
+            if (sp.kind == 1)
+                rj.push_back(tps_job(j->d_src, sp.src_sz, j->d_dst, sp.dst_sz, static_cast<const float4 *>(j->d_nodes),
+                                     sp.g, sp.dtype, sp.interp));
+            else
+                rj.push_back(affine_job(j->d_src, sp.src_sz, j->d_dst, sp.dst_sz, sp.M, sp.dtype, sp.interp));
+        }
+        TW_TRY(run_jobs(ctx, rj.data(), (int)rj.size(), s->batch));
+        cudaEvent_t done;
+        TW_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        TW_CUDA_TRY(cudaEventRecord(done, s->batch));
+        for (JobRec *j : kv.second) {
+            TW_CUDA_TRY(cudaStreamWaitEvent(j->st, done, 0));
+            TW_CUDA_TRY(cudaMemcpyAsync(j->spec.dst, j->d_dst, j->dst_b, cudaMemcpyDeviceToHost, j->st));
+            TW_CUDA_TRY(cudaEventRecord(j->ev_done, j->st));
+            j->state = kComputing;
+        }
+        cudaEventDestroy(done);  // destruction is deferred until the event completes
+    }
+    return TW_OK;
+}
+
+void finish(tw_server *s, JobRec *j, tw_status st)
+{
+    release(s, j);
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->status = st;
+    j->t_done = now_s();
+    j->state = kDone;
+    s->used -= j->reserve;
+    s->cv_done.notify_all();
+}
+
+void worker_main(tw_server *s)
+{
+    cudaSetDevice(s->ctx->device);
+    for (;;) {
+        bool progressed = false;
+        // 1. admission (FIFO, budget and in-flight bound)
+        for (;;) {
+            JobRec *j = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                if (s->queued.empty() || (int)s->active.size() >= s->max_inflight) break;
+                JobRec *h = s->queued.front();
+                if (s->used + h->reserve > s->budget && !s->active.empty()) break;  // wait for memory
+                s->queued.pop_front();
+                s->used += h->reserve;
+                j = h;
+            }
+            progressed = true;
+            if (j->reserve > s->budget) {
+                finish(s, j, TW_ERR_OOM);
+                continue;
+            }
+            tw_status st = prepare(s, j);
+            if (st != TW_OK) {
+                finish(s, j, st);
+                continue;
+            }
+            j->state = kPrepared;
+            s->active.push_back(j);
+        }
+        // 2. batch every prepared job whose inputs are on the device
+        std::vector<JobRec *> ready;
+        for (JobRec *j : s->active)
+            if (j->state == kPrepared && cudaEventQuery(j->ev_ready) == cudaSuccess) ready.push_back(j);
+        if (!ready.empty()) {
+            progressed = true;
+            tw_status st = batch_round(s, ready);
+            if (st != TW_OK)
+                for (JobRec *j : ready) j->status = st;
+        }
+        // 3. completion
+        for (size_t i = 0; i < s->active.size();) {
+            JobRec *j = s->active[i];
+            bool done = false;
+            tw_status st = TW_OK;
+            if (j->state == kComputing) {
+                cudaError_t e = cudaEventQuery(j->ev_done);
+                if (e == cudaSuccess) done = true;
+                else if (e != cudaErrorNotReady) { done = true; st = TW_ERR_CUDA; }
+            } else if (j->state == kPrepared && j->status != TW_ERR_NOT_READY) {
+                done = true;
+                st = j->status;
+            }
+            if (done) {
+                progressed = true;
+                finish(s, j, st);
+                s->active.erase(s->active.begin() + i);
+            } else {
+                ++i;
+            }
+        }
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (s->stop && s->queued.empty() && s->active.empty()) break;
+        if (!progressed) s->cv_work.wait_for(lk, std::chrono::microseconds(100));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+tw_status tw_server_create(tw_ctx *ctx, size_t hbm_budget_bytes, int max_inflight, tw_server **out)
+{
+    if (!ctx || !out) return TW_ERR_ARG;
+    *out = nullptr;
+    std::unique_ptr<tw_server> s(new tw_server);
+    TW_TRY(tw_ctx_create(ctx->device, 0, &s->ctx));
+    s->budget = hbm_budget_bytes ? hbm_budget_bytes : s->ctx->budget / 2;
+    s->max_inflight = max_inflight > 0 ? max_inflight : 16;
+    if (cudaStreamCreateWithFlags(&s->batch, cudaStreamNonBlocking) != cudaSuccess) {
+        tw_ctx_destroy(s->ctx);
+        return TW_ERR_CUDA;
+    }
+    s->worker = std::thread(worker_main, s.get());
+    *out = s.release();
+    return TW_OK;
+}
+
+tw_status tw_server_submit(tw_server *s, const tw_job *job, uint64_t *job_id)
+{
+    if (!s || !job || !job_id) return TW_ERR_ARG;
+    const tw_job &sp = *job;
+    if ((sp.dtype != TW_U8 && sp.dtype != TW_U16) || (sp.interp != 0 && sp.interp != 1) || !sp.src || !sp.dst)
+        return TW_ERR_ARG;
+    for (int a = 0; a < 3; ++a)
+        if (sp.src_sz[a] < 1 || sp.dst_sz[a] < 1) return TW_ERR_ARG;
+    if (sp.kind == 1) {
+        if (!g_supported(sp.g) || !sp.centres || !sp.values || sp.n < 4) return TW_ERR_ARG;
+    } else if (sp.kind != 0) {
+        return TW_ERR_ARG;
+    }
+    std::unique_ptr<JobRec> j(new JobRec);
+    j->spec = sp;
+    if (sp.kind == 1) {
+        j->ctr.assign(sp.centres, sp.centres + sp.n);
+        j->val.assign(sp.values, sp.values + sp.n);
+        j->spec.centres = j->ctr.data();
+        j->spec.values = j->val.data();
+    }
+    j->reserve = job_reserve(*j);
+    j->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return TW_ERR_ARG;
+    j->id = s->next_id++;
+    *job_id = j->id;
+    s->queued.push_back(j.get());
+    s->jobs[j->id] = std::move(j);
+    s->cv_work.notify_one();
+    return TW_OK;
+}
+
+tw_status tw_server_poll(tw_server *s, uint64_t job_id, double *latency_s)
+{
+    if (!s) return TW_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return TW_ERR_ARG;
+    JobRec *j = it->second.get();
+    if (j->state != kDone) return TW_ERR_NOT_READY;
+    if (latency_s) *latency_s = j->t_done - j->t_submit;
+    return j->status;
+}
+
+tw_status tw_server_wait(tw_server *s, uint64_t job_id, double timeout_s, double *latency_s)
+{
+    if (!s) return TW_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return TW_ERR_ARG;
+    JobRec *j = it->second.get();
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
+    while (j->state != kDone) {
+        if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && j->state != kDone)
+            return TW_ERR_TIMEOUT;
+    }
+    if (latency_s) *latency_s = j->t_done - j->t_submit;
+    return j->status;
+}
+
+tw_status tw_server_destroy(tw_server *s)
+{
+    if (!s) return TW_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->batch);
+    for (cudaStream_t st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    cudaStreamDestroy(s->batch);
+    tw_ctx_destroy(s->ctx);
+    delete s;
+    return TW_OK;
+}
+
+}  // extern "C"

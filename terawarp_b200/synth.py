@@ -163,6 +163,46 @@ def affine_landmarks(M, sz_xyz, n: int, seed: int, noise: float = 0.5, margin: f
 
 
 @dataclass
+class JobSpec:
+    kind: str            # "affine", "rigid" (rotation + translation) or "tps"
+    dtype: str           # "u8" or "u16"
+    shape_zyx: tuple
+    M: np.ndarray | None = None
+    centres: np.ndarray | None = None   # TPS centres (target-image landmarks)
+    values: np.ndarray | None = None    # TPS values (subject-image landmarks)
+    g: int = 16
+    arrival_s: float = 0.0
+
+
+def serving_jobs(n: int, seed: int = 1239, rate_hz: float = 20.0, dims_lo=(128, 128, 128),
+                 dims_hi=(1024, 1024, 256), n_lo: int = 16, n_hi: int = 4096, g: int = 16):
+    """The serving mix: Poisson arrivals at `rate_hz`, dims log-uniform per
+    axis between dims_lo and dims_hi (x, y, z), uint8/uint16 50/50, 30%
+    affine / 10% rotation+translation / 60% TPS with log-uniform landmark
+    counts and the smooth sinusoidal displacement model."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    jobs = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate_hz)
+        X, Y, Z = (int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))))) for lo, hi in zip(dims_lo, dims_hi))
+        dtype = "u8" if rng.random() < 0.5 else "u16"
+        u = rng.random()
+        if u < 0.3:
+            M = random_affine(int(rng.integers(1 << 30)), (X, Y, Z))
+            jobs.append(JobSpec("affine", dtype, (Z, Y, X), M=M, arrival_s=t))
+        elif u < 0.4:
+            # rotation (up to 30 degrees per axis) about the centre + translation
+            M = random_affine(int(rng.integers(1 << 30)), (X, Y, Z), rot_deg=30.0, scale=(1.0, 1.0), trans=20.0)
+            jobs.append(JobSpec("rigid", dtype, (Z, Y, X), M=M, arrival_s=t))
+        else:
+            nl = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+            sub, tar = lattice_landmarks((X, Y, Z), nl, int(rng.integers(1 << 30)), margin=min(8.0, min(X, Y, Z) / 8))
+            jobs.append(JobSpec("tps", dtype, (Z, Y, X), centres=tar, values=sub, g=g, arrival_s=t))
+    return jobs
+
+
+@dataclass
 class Case:
     name: str
     vol: object          # torch tensor (z, y, x)
