@@ -82,7 +82,9 @@ class Clocks:
                                        "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
-        time.sleep(0.3)
+        # nvidia-smi's own start-up (NVML initialisation) disturbs the GPU for a
+        # moment; let it finish before the timed region begins.
+        time.sleep(2.0)
         return self
 
     def __exit__(self, *a):
@@ -290,6 +292,7 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
         "stages_ms": {"solve_fp64": statistics.mean(solve_ms), "node_eval_fp32": eval_avg, "resample": warp_avg},
+        "resample_ms_per_step": [round(v, 3) for v in warp_ms],
         "tps_eval": {"pairs": pairs, "flop_per_pair": 15, "tflops": pairs * 15 / (eval_avg / 1e3) / 1e12,
                      "fp32_peak_tflops_at_clock": fp32_peak_tflops,
                      "frac": pairs * 15 / (eval_avg / 1e3) / 1e12 / fp32_peak_tflops},

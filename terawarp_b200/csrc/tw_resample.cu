@@ -310,45 +310,302 @@ __device__ __forceinline__ void store_pair(T *p, uint32_t v0, uint32_t v1, bool 
     }
 }
 
+// ---------------------------------------------------------------- packed FP32x2
+// Blackwell issues two FP32 operations per instruction (FFMA2/FADD2).  The
+// unchecked path of a lane's voxel pair is written in pairs: the B-spline
+// taps as (x, y) per voxel and (z0, z1) across the pair (Q stores z twice),
+// floor/frac on the same pairs, and the trilinear lerps across the pair.
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as one FFMA2 (b * -1 + a, a single rounding, so exact like a
+// subtraction); negating both lanes first would cost two logic ops
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+
+// Packs the low halfword (u16) or byte (u8) of two words: voxel pair x, x+1.
+template <typename T>
+__device__ __forceinline__ uint32_t pack_pair(uint32_t a, uint32_t b)
+{
+    return sizeof(T) == 2 ? __byte_perm(a, b, 0x5410) : __byte_perm(a, b, 0x0040);
+}
+
+// Stores a packed voxel pair: one 2-element store when aligned, else per
+// element within the row's valid extent.
+template <typename T>
+__device__ __forceinline__ void store_packed(T *p, uint32_t w, bool pair_ok, int nvalid)
+{
+    if (pair_ok && nvalid >= 2) {
+        if (sizeof(T) == 2) *reinterpret_cast<uint32_t *>(p) = w;
+        else *reinterpret_cast<uint16_t *>(p) = (uint16_t)w;
+    } else {
+        const int sh = 8 * (int)sizeof(T);
+        if (nvalid >= 1) p[0] = (T)(w & ((1u << sh) - 1u));
+        if (nvalid >= 2) p[1] = (T)((w >> sh) & ((1u << sh) - 1u));
+    }
+}
+
+// Magic float 2^23 + v for a loaded voxel value v (exact for v < 2^23).
+template <typename T>
+__device__ __forceinline__ float mag(const T *p)
+{
+    return __int_as_float(0x4B000000 | (int)(uint32_t)__ldg(p));
+}
+
+// Per-lane constants of the packed path: weight pairs for the two voxels.
+struct PairW {
+    float2 w0[4];  // (w_a(0), w_a(0))
+    float2 w1[4];  // (w_a(1), w_a(1))
+    float2 wz[4];  // (w_a(0), w_a(1))
+};
+
+__device__ __forceinline__ PairW make_pairw(const float4 (&wx)[2])
+{
+    PairW p;
+    const float a0[4] = {wx[0].x, wx[0].y, wx[0].z, wx[0].w};
+    const float a1[4] = {wx[1].x, wx[1].y, wx[1].z, wx[1].w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        p.w0[a] = f2(a0[a], a0[a]);
+        p.w1[a] = f2(a1[a], a1[a]);
+        p.wz[a] = f2(a0[a], a1[a]);
+    }
+    return p;
+}
+
+// Sample positions of a TPS voxel pair from its 4 x-taps: (qx, qy) of voxel
+// 0 and of voxel 1, and (qz0, qz1).
+__device__ __forceinline__ void pair_positions(const float4 n[4], const PairW &pw, float2 &p0, float2 &p1, float2 &pz2)
+{
+    p0 = make_float2(0.f, 0.f);
+    p1 = p0;
+    pz2 = p0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const float2 xy = f2(n[a].x, n[a].y);
+        const float2 zz = f2(n[a].z, n[a].w);  // Q stores (x, y, z, z)
+        p0 = fma2(pw.w0[a], xy, p0);
+        p1 = fma2(pw.w1[a], xy, p1);
+        pz2 = fma2(pw.wz[a], zz, pz2);
+    }
+}
+
+// The four source rows a trilinear sample reads, (dy, dz) = (r & 1, r >> 1),
+// as base pointers of one brick, plus the int32 pitches: a tap address is
+// then one wide multiply-add of a 32-bit offset onto a row base.
+template <typename T>
+struct Rows {
+    const T *rb[4];
+    int py, pz;
+    uint32_t k;  // magic-number bias folded out of the offsets
+};
+
+template <typename T>
+__device__ __forceinline__ Rows<T> make_rows(const T *base, int py, int pz)
+{
+    Rows<T> r;
+    r.rb[0] = base;
+    r.rb[1] = base + py;
+    r.rb[2] = base + pz;
+    r.rb[3] = base + pz + py;
+    r.py = py;
+    r.pz = pz;
+    r.k = (uint32_t)kMagicBits * (uint32_t)(pz + py + 1);
+    return r;
+}
+
+// Element offset of floor(q) from the magic-floor bit patterns (2^32 wrap
+// arithmetic; the result is the exact offset because it fits int32).
+template <typename T>
+__device__ __forceinline__ int tap_offset(const Rows<T> &R, float mx, float my, float mz)
+{
+    const uint32_t o = (uint32_t)__float_as_int(mz) * (uint32_t)R.pz + (uint32_t)__float_as_int(my) * (uint32_t)R.py +
+                       (uint32_t)__float_as_int(mx) - R.k;
+    return (int)o;
+}
+
+// Unchecked sample of a voxel pair at positions (p0, p1, pz2): every tap is
+// known to be inside the volume and the buffer (hull test), offsets fit int32.
+template <typename T, bool ROUND>
+__device__ __forceinline__ void pair_fast2(float2 p0, float2 p1, float2 pz2, const Rows<T> &R, uint32_t &packed)
+{
+    const float2 MM = f2(kMagic, kMagic);
+    // floor via add.rm of 1.5*2^23, fractions
+    const float2 m0 = __fadd2_rd(p0, MM), m1 = __fadd2_rd(p1, MM), mz = __fadd2_rd(pz2, MM);
+    const float2 f0 = sub2(p0, sub2(m0, MM)), f1 = sub2(p1, sub2(m1, MM)), fz = sub2(pz2, sub2(mz, MM));
+    const int off0 = tap_offset(R, m0.x, m0.y, mz.x);
+    const int off1 = tap_offset(R, m1.x, m1.y, mz.y);
+    // magic floats of the 8 taps of both voxels
+    float2 lo[4], hi[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const T *q0 = R.rb[r] + off0, *q1 = R.rb[r] + off1;
+        lo[r] = f2(mag(q0), mag(q1));
+        hi[r] = f2(mag(q0 + 1), mag(q1 + 1));
+    }
+    const float2 fx = f2(f0.x, f1.x), fy = f2(f0.y, f1.y);
+    float2 ax[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)  // (2^23 + b) - (2^23 + a) = b - a exactly
+        ax[r] = fma2(fx, sub2(hi[r], lo[r]), sub2(lo[r], f2(8388608.f, 8388608.f)));
+    const float2 b0 = fma2(fy, sub2(ax[1], ax[0]), ax[0]);
+    const float2 b1 = fma2(fy, sub2(ax[3], ax[2]), ax[2]);
+    float2 v = fma2(fz, sub2(b1, b0), b0);
+    // v is a convex combination of voxel values; rounding can leave -0.0x
+    if (ROUND) v = add2(v, f2(0.5f, 0.5f));
+    else v = f2(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f));
+    // 2^23 + floor(v): floor(v) lies in [0, max of T] (v never exceeds the
+    // largest tap by more than an ulp), so its low bits are the output
+    const float2 t = __fadd2_rd(v, f2(8388608.f, 8388608.f));
+    packed = pack_pair<T>(__float_as_uint(t.x), __float_as_uint(t.y));
+}
+
+// Checked sample of a voxel pair near the volume or buffer border: the same
+// packed arithmetic, plus the reference's range test per voxel (0 <= q <=
+// sz-1, else 0) and taps clamped to [cl, ch] (the source buffer, narrowed to
+// the brick's sample hull so that offsets stay 32-bit).  A tap clamped away
+// from floor(q)+1 only happens where its weight is 0 (q integral at sz-1).
+template <typename T, bool ROUND, typename OFF>
+__device__ __forceinline__ void pair_checked2(float2 p0, float2 p1, float2 pz2, const T *__restrict__ base, OFF py,
+                                              OFF pz, const Frame &f, const int (&cl)[3], const int (&ch)[3],
+                                              int nvalid, uint32_t &packed)
+{
+    const float2 MM = f2(kMagic, kMagic);
+    const bool ok0 = nvalid >= 1 && p0.x >= f.lo[0] && p0.x <= f.hi[0] && p0.y >= f.lo[1] && p0.y <= f.hi[1] &&
+                     pz2.x >= f.lo[2] && pz2.x <= f.hi[2];
+    const bool ok1 = nvalid >= 2 && p1.x >= f.lo[0] && p1.x <= f.hi[0] && p1.y >= f.lo[1] && p1.y <= f.hi[1] &&
+                     pz2.y >= f.lo[2] && pz2.y <= f.hi[2];
+    // positions of rejected voxels are replaced by the frame's low corner so
+    // that the magic floor below stays exact (NaN or far-away q)
+    if (!ok0) { p0 = f2(f.lo[0], f.lo[1]); pz2.x = f.lo[2]; }
+    if (!ok1) { p1 = f2(f.lo[0], f.lo[1]); pz2.y = f.lo[2]; }
+    const float2 m0 = __fadd2_rd(p0, MM), m1 = __fadd2_rd(p1, MM), mz = __fadd2_rd(pz2, MM);
+    const float2 f0 = sub2(p0, sub2(m0, MM)), f1 = sub2(p1, sub2(m1, MM)), fz = sub2(pz2, sub2(mz, MM));
+    const int ix0 = __float_as_int(m0.x) - kMagicBits, iy0 = __float_as_int(m0.y) - kMagicBits;
+    const int ix1 = __float_as_int(m1.x) - kMagicBits, iy1 = __float_as_int(m1.y) - kMagicBits;
+    const int iz0 = __float_as_int(mz.x) - kMagicBits, iz1 = __float_as_int(mz.y) - kMagicBits;
+    const int xa0 = clampi(ix0, cl[0], ch[0]), xb0 = clampi(ix0 + 1, cl[0], ch[0]);
+    const int xa1 = clampi(ix1, cl[0], ch[0]), xb1 = clampi(ix1 + 1, cl[0], ch[0]);
+    const int ya0 = clampi(iy0, cl[1], ch[1]), yb0 = clampi(iy0 + 1, cl[1], ch[1]);
+    const int ya1 = clampi(iy1, cl[1], ch[1]), yb1 = clampi(iy1 + 1, cl[1], ch[1]);
+    const int za0 = clampi(iz0, cl[2], ch[2]), zb0 = clampi(iz0 + 1, cl[2], ch[2]);
+    const int za1 = clampi(iz1, cl[2], ch[2]), zb1 = clampi(iz1 + 1, cl[2], ch[2]);
+    const int ys0[2] = {ya0, yb0}, ys1[2] = {ya1, yb1}, zs0[2] = {za0, zb0}, zs1[2] = {za1, zb1};
+    float2 lo[4], hi[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const T *r0 = base + ((OFF)zs0[r >> 1] * pz + (OFF)ys0[r & 1] * py);
+        const T *r1 = base + ((OFF)zs1[r >> 1] * pz + (OFF)ys1[r & 1] * py);
+        lo[r] = f2(mag(r0 + xa0), mag(r1 + xa1));
+        hi[r] = f2(mag(r0 + xb0), mag(r1 + xb1));
+    }
+    const float2 fx = f2(f0.x, f1.x), fy = f2(f0.y, f1.y);
+    float2 ax[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) ax[r] = fma2(fx, sub2(hi[r], lo[r]), sub2(lo[r], f2(8388608.f, 8388608.f)));
+    const float2 b0 = fma2(fy, sub2(ax[1], ax[0]), ax[0]);
+    const float2 b1 = fma2(fy, sub2(ax[3], ax[2]), ax[2]);
+    float2 v = fma2(fz, sub2(b1, b0), b0);
+    if (ROUND) v = add2(v, f2(0.5f, 0.5f));
+    else v = f2(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f));
+    const float2 t = __fadd2_rd(v, f2(8388608.f, 8388608.f));
+    // a rejected voxel writes 0: the bits of 2^23 have zero low bits
+    packed = pack_pair<T>(ok0 ? __float_as_uint(t.x) : 0x4B000000u, ok1 ? __float_as_uint(t.y) : 0x4B000000u);
+}
+
 // One output slice of a brick.  Lane l of warp w owns voxel pairs
 // (x, x+1), x = 2l + 64k (k = 0..3), of rows y = w + 8r: a warp's gathers
 // then cover 64 consecutive voxels (about one 128-byte line per tap) instead
 // of 256.  The pair shares one cell (G >= 2), its 4 node taps come from Q
 // (z/y-contracted nodes), and the x expansion is 12 FMA per voxel.
+// Clamp window of a brick's checked taps: the source buffer narrowed to the
+// brick's sample hull (+1), and whether offsets inside it fit int32.
+struct Clamp {
+    int cl[3], ch[3];
+    bool span32;
+};
+
+__device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const float (&mn)[3], const float (&mx)[3])
+{
+    Clamp c;
+    double span = 0.0;
+    const double pitch[3] = {1.0, (double)J.src_py, (double)J.src_pz};
+    for (int a = 0; a < 3; ++a) {
+        const double lo = fmax(-1.0e9, fmin(1.0e9, floor((double)mn[a]) - 1.0));
+        const double hi = fmax(-1.0e9, fmin(1.0e9, floor((double)mx[a]) + 2.0));
+        int l = max(f.bl[a], (int)lo), h = min(f.bh[a], (int)hi);
+        if (l > h) l = h = f.bl[a];  // no sample can be valid here; any in-buffer tap will do
+        c.cl[a] = l;
+        c.ch[a] = h;
+        span += fmax(fabs((double)l), fabs((double)h)) * pitch[a];
+    }
+    c.span32 = span < 1.0e9 && J.src_pz < 0x3fffffff;
+    return c;
+}
+
+// Everything a lane needs about its brick, computed once per brick.
+template <typename T>
+struct BrickCtx {
+    const T *base;      // source element at the frame origin (may lie outside the buffer)
+    int py32, pz32;     // source pitches as int (valid when the brick's offsets fit int32)
+    int64_t py, pz;     // source pitches
+    Frame frame;
+    Clamp cw;
+    Rows<T> rows;
+    PairW pw;           // packed x weights of the lane's voxel pair
+    float4 wx[2];       // scalar x weights (nearest-neighbour path)
+    bool pair_ok;       // a voxel pair can be stored as one 2-element word
+    int xe;             // valid x extent of the brick's output region
+};
+
 template <typename T, int G, int INTERP>
-__device__ __forceinline__ void tps_pair(const float4 *Q, const float4 (&wx)[2], int y, int x, bool fast, int xe,
-                                         const T *base, int py32, int pz32, int64_t py, int64_t pz,
-                                         const Frame &frame, T *drow, bool pair_ok)
+__device__ __forceinline__ void tps_pair(const float4 *Q, const BrickCtx<T> &B, int y, int x, bool fast, T *drow)
 {
     using Gm = Geom<G>;
     const float4 *qn = Q + y * Gm::NX + x / G;
     const float4 n0 = qn[0], n1 = qn[1], n2 = qn[2], n3 = qn[3];
     uint32_t outv[2];
+    if (INTERP == 0) {
+        const float4 n[4] = {n0, n1, n2, n3};
+        float2 p0, p1, pz2;
+        pair_positions(n, B.pw, p0, p1, pz2);
+        uint32_t w;
+        if (fast) {
+            pair_fast2<T, true>(p0, p1, pz2, B.rows, w);
+            store_packed<T>(drow + x, w, B.pair_ok, 2);
+        } else {
+            const int nv = B.xe - x;
+            if (B.cw.span32)
+                pair_checked2<T, true, int>(p0, p1, pz2, B.base, B.py32, B.pz32, B.frame, B.cw.cl, B.cw.ch, nv, w);
+            else
+                pair_checked2<T, true, int64_t>(p0, p1, pz2, B.base, B.py, B.pz, B.frame, B.cw.cl, B.cw.ch, nv, w);
+            store_packed<T>(drow + x, w, B.pair_ok, nv);
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-        const float4 w = wx[j];
+        const float4 w = B.wx[j];
         const float qx = fmaf(w.x, n0.x, fmaf(w.y, n1.x, fmaf(w.z, n2.x, w.w * n3.x)));
         const float qy = fmaf(w.x, n0.y, fmaf(w.y, n1.y, fmaf(w.z, n2.y, w.w * n3.y)));
         const float qz = fmaf(w.x, n0.z, fmaf(w.y, n1.z, fmaf(w.z, n2.z, w.w * n3.z)));
         float v;
         if (fast) {
-            v = sample_fast<T, INTERP>(base, py32, pz32, qx, qy, qz);
+            v = sample_fast<T, INTERP>(B.base, B.py32, B.pz32, qx, qy, qz);
             outv[j] = INTERP == 1 ? (uint32_t)v : to_out<T, true>(v);
         } else {
-            const bool ok = (x + j) < xe && sample_checked<T, INTERP>(base, py, pz, frame, qx, qy, qz, v);
+            const bool ok = (x + j) < B.xe && sample_checked<T, INTERP>(B.base, B.py, B.pz, B.frame, qx, qy, qz, v);
             outv[j] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, true>(v)) : 0u;
         }
     }
-    store_pair<T>(drow + x, outv[0], outv[1], pair_ok, fast ? 2 : xe - x);
+    store_pair<T>(drow + x, outv[0], outv[1], B.pair_ok, fast ? 2 : B.xe - x);
 }
 
 // ALL_FAST: the whole brick is inside; else segf[y*4 + k] says whether the
 // warp-row segment (row y, voxels 64k..64k+63) may skip the bounds checks.
 template <typename T, int G, int INTERP, bool ALL_FAST>
-__device__ __forceinline__ void tps_rows(const float4 *Q, const float4 (&wx)[2], int lane, int ty, int ye, int xe,
-                                         const T *base, int py32, int pz32, int64_t py, int64_t pz,
-                                         const Frame &frame, T *dslice, int64_t dpy, bool pair_ok,
-                                         const unsigned char *segf)
+__device__ __forceinline__ void tps_rows(const float4 *Q, const BrickCtx<T> &B, int lane, int ty, int ye, T *dslice,
+                                         int64_t dpy, const unsigned char *segf)
 {
     using Gm = Geom<G>;
 #pragma unroll 1
@@ -360,11 +617,11 @@ __device__ __forceinline__ void tps_rows(const float4 *Q, const float4 (&wx)[2],
         for (int k = 0; k < Gm::BX / 64; ++k) {
             const int x = 2 * lane + 64 * k;
             if (ALL_FAST) {
-                tps_pair<T, G, INTERP>(Q, wx, y, x, true, xe, base, py32, pz32, py, pz, frame, drow, pair_ok);
+                tps_pair<T, G, INTERP>(Q, B, y, x, true, drow);
             } else if (segf[y * 4 + k]) {  // warp-uniform
-                tps_pair<T, G, INTERP>(Q, wx, y, x, true, xe, base, py32, pz32, py, pz, frame, drow, pair_ok);
-            } else if (x < xe) {
-                tps_pair<T, G, INTERP>(Q, wx, y, x, false, xe, base, py32, pz32, py, pz, frame, drow, pair_ok);
+                tps_pair<T, G, INTERP>(Q, B, y, x, true, drow);
+            } else if (x < B.xe) {
+                tps_pair<T, G, INTERP>(Q, B, y, x, false, drow);
             }
         }
     }
@@ -427,6 +684,7 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     const bool fast = inside_out && hull_inside(J, O, mn, mx);
     const Frame frame = make_frame(J, O);
     const bool span_ok = offsets_fit_32(J, mn, mx);
+    const Clamp cw = make_clamp(J, frame, mn, mx);
 
     // 2. R[y][c][nx] = sum_b wy_b(y) Nd[c][y/G + b][nx]
     for (int i = tid; i < Gm::NR; i += kThreads) {
@@ -472,22 +730,28 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     }
     __syncthreads();
 
-    // x weights of the lane's voxel pair (2l, 2l+1) + 64k: the brick origin is
-    // a multiple of G and G divides 64, so they do not depend on k
-    float4 wx[2];
-    wx[0] = W[(2 * tx) % G];
-    wx[1] = W[(2 * tx + 1) % G];
-
     const T *src = static_cast<const T *>(J.src);
     T *dst = static_cast<T *>(J.dst);
     const int64_t sbase = (O[2] - J.src_o[2]) * J.src_pz + (O[1] - J.src_o[1]) * J.src_py + (O[0] - J.src_o[0]);
-    const T *base = src + sbase;
-    const int py32 = (int)J.src_py, pz32 = (int)J.src_pz;
     // output plane z of the loop below is zfirst + z
     const int64_t dbase0 = (zfirst - J.out_o[2]) * J.dst_pz + (O[1] - J.out_o[1]) * J.dst_py + (O[0] - J.out_o[0]);
+    BrickCtx<T> B;
+    B.base = src + sbase;
+    B.py32 = (int)J.src_py;
+    B.pz32 = (int)J.src_pz;
+    B.py = J.src_py;
+    B.pz = J.src_pz;
+    B.frame = frame;
+    B.cw = cw;
+    B.rows = make_rows(B.base, B.py32, B.pz32);
+    // x weights of the lane's voxel pair (2l, 2l+1) + 64k: the brick origin is
+    // a multiple of G and G divides 64, so they do not depend on k
+    B.wx[0] = W[(2 * tx) % G];
+    B.wx[1] = W[(2 * tx + 1) % G];
+    B.pw = make_pairw(B.wx);
     // a voxel pair (even x) can be written as one 2-element store
-    const bool pair_ok = ((((uintptr_t)(dst + dbase0)) % (2 * sizeof(T))) == 0) && (J.dst_py % 2 == 0) &&
-                         (J.dst_pz % 2 == 0);
+    B.pair_ok = ((((uintptr_t)(dst + dbase0)) % (2 * sizeof(T))) == 0) && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
+    B.xe = (int)xe;
     const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
     const int64_t ze = J.out_o[2] + J.out_n[2] - zfirst;
 
@@ -502,20 +766,17 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
             q.x = fmaf(wz.x, a.x, fmaf(wz.y, b.x, fmaf(wz.z, e.x, wz.w * f.x)));
             q.y = fmaf(wz.x, a.y, fmaf(wz.y, b.y, fmaf(wz.z, e.y, wz.w * f.y)));
             q.z = fmaf(wz.x, a.z, fmaf(wz.y, b.z, fmaf(wz.z, e.z, wz.w * f.z)));
-            q.w = 0.f;
+            q.w = q.z;  // z twice: the packed path reads (z, z) as one pair
             Q[i] = q;
         }
         __syncthreads();
         if (z >= ze) continue;  // uniform: whole slice outside the region
         // fast bricks skip the per-segment flags; otherwise each warp-row
         // segment picks its path (uniform across the warp)
-        if (fast) {
-            tps_rows<T, G, INTERP, true>(Q, wx, tx, ty, (int)ye, (int)xe, base, py32, pz32, J.src_py, J.src_pz, frame,
-                                          dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, pair_ok, segf);
-        } else {
-            tps_rows<T, G, INTERP, false>(Q, wx, tx, ty, (int)ye, (int)xe, base, py32, pz32, J.src_py, J.src_pz,
-                                           frame, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, pair_ok, segf);
-        }
+        if (fast)
+            tps_rows<T, G, INTERP, true>(Q, B, tx, ty, (int)ye, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, segf);
+        else
+            tps_rows<T, G, INTERP, false>(Q, B, tx, ty, (int)ye, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, segf);
     }
     __syncthreads();  // smem reuse by the next brick
 }
@@ -529,7 +790,8 @@ constexpr int kABY = 8, kABZ = 8;
 template <typename T, int INTERP, bool FAST>
 __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float (&fo)[3], int lane, int ty, int ye,
                                             int ze, int xe, const T *base, int py32, int pz32, int64_t py, int64_t pz,
-                                            const Frame &frame, T *dbrick, int64_t dpy, int64_t dpz, bool pair_ok)
+                                            const Frame &frame, const Clamp &cw, T *dbrick, int64_t dpy, int64_t dpz,
+                                            bool pair_ok)
 {
 #pragma unroll 1
     for (int z = 0; z < kABZ; ++z) {
@@ -545,6 +807,22 @@ __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float 
             const int x = 2 * lane + 64 * k;
             if (!FAST && x >= xe) continue;
             uint32_t outv[2];
+            if (INTERP == 0) {  // packed pair path, truncation (no +0.5)
+                const float lx = (float)x;
+                const float2 p0 = f2(fmaf(m[0][0], lx, bx0), fmaf(m[1][0], lx, by0));
+                const float2 p1 = add2(p0, f2(m[0][0], m[1][0]));
+                const float qz0 = fmaf(m[2][0], lx, bz0);
+                const float2 pz2 = f2(qz0, qz0 + m[2][0]);
+                uint32_t w;
+                if (FAST)
+                    pair_fast2<T, false>(p0, p1, pz2, make_rows(base, py32, pz32), w);
+                else if (cw.span32)
+                    pair_checked2<T, false, int>(p0, p1, pz2, base, py32, pz32, frame, cw.cl, cw.ch, xe - x, w);
+                else
+                    pair_checked2<T, false, int64_t>(p0, p1, pz2, base, py, pz, frame, cw.cl, cw.ch, xe - x, w);
+                store_packed<T>(drow + x, w, pair_ok, FAST ? 2 : xe - x);
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 const float lx = (float)(x + j);
@@ -616,12 +894,13 @@ __device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, 
     const int64_t xe = J.out_o[0] + J.out_n[0] - O[0];
     const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
     const int64_t ze = J.out_o[2] + J.out_n[2] - O[2];
+    const Clamp cw = make_clamp(J, frame, lo, hi);
     if (fast)
         affine_rows<T, INTERP, true>(m, fo, tx, ty, (int)ye, (int)ze, (int)xe, base, py32, pz32, J.src_py, J.src_pz,
-                                     frame, dst + dbase0, J.dst_py, J.dst_pz, pair_ok);
+                                     frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok);
     else
         affine_rows<T, INTERP, false>(m, fo, tx, ty, (int)ye, (int)ze, (int)xe, base, py32, pz32, J.src_py, J.src_pz,
-                                      frame, dst + dbase0, J.dst_py, J.dst_pz, pair_ok);
+                                      frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok);
 }
 
 // ---------------------------------------------------------------- kernels
