@@ -123,6 +123,29 @@ tw_status tw_warp_tps_device(tw_ctx *ctx, const void *dev_nodes, int g, int dtyp
  * coordinates. */
 tw_status tw_fit_affine(tw_ctx *ctx, const tw_marker *tar, const tw_marker *sub, int n, double M[16]);
 
+/* Largest n accepted by tw_fit_affine_noalloc. */
+#define TW_FIT_AFFINE_NOALLOC_MAX 4096
+
+/* tw_fit_affine without allocating: no device memory is allocated, and on the
+ * host nothing but the message of a failed call.  No counterpart in the
+ * reference: it exists for callers that cannot allocate at the time they
+ * fit, e.g. a process whose device memory is wholly reserved by its own
+ * volume cache or by this context's HBM budget (tw_fit_affine would then fail
+ * with TW_ERR_OOM), or a loop that must not let an allocation wait on, or
+ * stall, warps running on other streams.
+ *
+ * Its scratch is one fixed array in device memory per device (about 288 KiB,
+ * reserved by the CUDA driver when it loads this entry point's device code on
+ * that device), so n is limited to TW_FIT_AFFINE_NOALLOC_MAX; larger n
+ * returns TW_ERR_ARG.
+ * Same kernel, same FP64 arithmetic and same result as tw_fit_affine.
+ * Calls that overlapped on the GPU would race on that one array, so calls for
+ * the same device are serialised by a lock inside the library.  The first
+ * call on each device looks up the array's address (and may load the device
+ * code); make it before any stream capture begins.  Synchronises ctx's
+ * stream. */
+tw_status tw_fit_affine_noalloc(tw_ctx *ctx, const tw_marker *tar, const tw_marker *sub, int n, double M[16]);
+
 /* Builds the pull-back matrix of the TeraWarp command's parameter surface
  * (README.md:85-100), for which the reference source has no code:
  *   warp_mode 0 (non-rigid), deformation_mode 2 (scaling): para = per-axis

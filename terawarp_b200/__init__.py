@@ -7,11 +7,11 @@ pinned double-buffered host<->HBM streaming, behind a C ABI
 the reference's operator functions over that ABI.
 """
 from .api import (Context, TeraWarpError, TPS, bigimagewarp, downsample_factor, downsample_image, fit_affine,
-                  grid_size, imgwarp_smallmemory_image, make_affine, output_size, params, q_imagewarp_affine_image,
+                  fit_affine_noalloc, grid_size, imgwarp_smallmemory_image, make_affine, output_size, params, q_imagewarp_affine_image,
                   tps_eval_grid, tps_solve, warp_affine_device, warp_tps_device)
 
 __all__ = [
     "Context", "TeraWarpError", "TPS", "bigimagewarp", "downsample_factor", "downsample_image", "fit_affine",
-    "grid_size", "imgwarp_smallmemory_image", "make_affine", "output_size", "params", "q_imagewarp_affine_image",
+    "fit_affine_noalloc", "grid_size", "imgwarp_smallmemory_image", "make_affine", "output_size", "params", "q_imagewarp_affine_image",
     "tps_eval_grid", "tps_solve", "warp_affine_device", "warp_tps_device",
 ]

@@ -74,6 +74,7 @@ SIGNATURES = {
     "tw_grid_size": (C.c_int64, [C.c_int64, C.c_int]),
     "tw_warp_tps_device": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P, _I64P, _P]),
     "tw_fit_affine": (C.c_int, [_P, _MP, _MP, C.c_int, _DP]),
+    "tw_fit_affine_noalloc": (C.c_int, [_P, _MP, _MP, C.c_int, _DP]),
     "tw_make_affine": (C.c_int, [C.c_int, C.c_int, _DP, _I64P, _I64P, _DP]),
     "tw_warp_affine_device": (C.c_int, [_P, _DP, C.c_int, C.c_int, _P, _I64P, _P, _I64P, _P]),
     "tw_imgwarp_smallmemory_image": (C.c_int, [_P, _MP, _MP, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_int,

@@ -206,6 +206,19 @@ def fit_affine(ctx: Context, tar, sub) -> np.ndarray:
     return M.reshape(4, 4)
 
 
+FIT_AFFINE_NOALLOC_MAX = 4096
+
+
+def fit_affine_noalloc(ctx: Context, tar, sub) -> np.ndarray:
+    """fit_affine through tw_fit_affine_noalloc: same result, no allocation;
+    at most FIT_AFFINE_NOALLOC_MAX landmark pairs."""
+    M = np.zeros(16, np.float64)
+    n = len(np.asarray(tar).reshape(-1, 3))
+    _check(ctx.lib.tw_fit_affine_noalloc(ctx.handle, _markers(tar), _markers(sub), n, M.ctypes.data_as(L._DP)),
+           ctx, "tw_fit_affine_noalloc")
+    return M.reshape(4, 4)
+
+
 def make_affine(warp_mode: int, deformation_mode: int, para, in_sz, out_sz=None) -> np.ndarray:
     """Pull-back matrix of the scaling / rotation / translation parameters."""
     out_sz = in_sz if out_sz is None else out_sz

@@ -90,6 +90,10 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
                            cudaStream_t st);
 tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_sub, int n, double M[16],
                             cudaStream_t st);
+// The affine fit kernel alone on caller-provided device buffers (d_status
+// must hold 0 when it starts; the kernel only sets failure bits).
+cudaError_t launch_affine_fit(const double *d_tar, const double *d_sub, int n, double *d_out, int *d_status,
+                              cudaStream_t st);
 
 // --------------------------------------------------------------- helpers
 

@@ -667,4 +667,11 @@ tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_su
     return TW_OK;
 }
 
+cudaError_t launch_affine_fit(const double *d_tar, const double *d_sub, int n, double *d_out, int *d_status,
+                              cudaStream_t st)
+{
+    k_affine_fit<<<1, 256, 0, st>>>(d_tar, d_sub, n, d_out, d_status);
+    return cudaGetLastError();
+}
+
 }  // namespace tw
