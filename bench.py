@@ -24,6 +24,7 @@ replica (the path needs no collective); value = all ranks' voxels / max time.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -66,15 +67,21 @@ def measured_peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling that covers the timed region.
+
+    The sampler starts before the warm-up steps: nvidia-smi's own start-up
+    (NVML initialisation) can stall the GPU for a moment, and that must not
+    land inside the timed region.  mark_start() / mark_end() bracket the timed
+    region; summary() keeps the samples taken inside it."""
 
     def __init__(self, index: int):
         self.index = index
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
@@ -82,10 +89,13 @@ class Clocks:
                                        "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
-        # nvidia-smi's own start-up (NVML initialisation) disturbs the GPU for a
-        # moment; let it finish before the timed region begins.
-        time.sleep(2.0)
         return self
+
+    def mark_start(self):
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        self.t1 = datetime.datetime.now()
 
     def __exit__(self, *a):
         if self.p:
@@ -98,19 +108,24 @@ class Clocks:
     def summary(self):
         self.f.flush()
         rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
-        sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        parsed = []
         for r in rows:
             try:
-                sm.append(float(r[1].split()[0]))
-                mx = max(mx, float(r[2].split()[0]))
-                for nm, v in zip(names, r[5:9]):
-                    if "Active" in v and "Not" not in v:
-                        reasons.add(nm)
+                ts = datetime.datetime.strptime(r[0].strip(), "%Y/%m/%d %H:%M:%S.%f")
+                parsed.append((ts, float(r[1].split()[0]), float(r[2].split()[0]),
+                               [nm for nm, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v]))
             except (ValueError, IndexError):
                 continue
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = parsed
+        if self.t0 is not None and self.t1 is not None:
+            pad = datetime.timedelta(seconds=0.25)
+            inside = [x for x in parsed if self.t0 - pad <= x[0] <= self.t1 + pad] or parsed
+        sm = [x[1] for x in inside]
+        reasons = sorted({nm for x in inside for nm in x[3]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max((x[2] for x in inside), default=None),
+                "reasons": reasons, "samples": len(sm)}
 
 
 def dist_init():
@@ -238,20 +253,27 @@ def run_ours(args):
             ev[2].record()
         return t
 
-    for _ in range(args.warmup):
-        step().close()
-    torch.cuda.synchronize()
-    launches0 = ctx.kernel_launches
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     keep = []
-    barrier(ws)
-    torch.cuda.synchronize()
     with Clocks(local) as clk:
+        t_warm = time.perf_counter()
+        for _ in range(args.warmup):
+            step().close()
+        torch.cuda.synchronize()
+        # warm-up lasts at least 2 s so that the sampler's start-up is over
+        while time.perf_counter() - t_warm < 2.0:
+            step().close()
+            torch.cuda.synchronize()
+        launches0 = ctx.kernel_launches
+        barrier(ws)
+        torch.cuda.synchronize()
+        clk.mark_start()
         for i in range(args.steps):
             evs[i][3].record()
             keep.append(step(evs[i][:3]))
         torch.cuda.synchronize()
         barrier(ws)
+        clk.mark_end()
     launches = ctx.kernel_launches - launches0
     for t in keep:
         t.close()

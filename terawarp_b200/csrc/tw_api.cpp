@@ -198,6 +198,13 @@ const char *tw_status_string(tw_status s)
 
 int tw_abi_version(void) { return TW_ABI_VERSION; }
 
+static tw_status destroy_partial(tw_ctx *c)
+{
+    cudaGetLastError();
+    tw_ctx_destroy(c);
+    return TW_ERR_CUDA;
+}
+
 tw_status tw_ctx_create(int device, size_t hbm_budget_bytes, tw_ctx **out)
 {
     if (!out) return TW_ERR_ARG;
@@ -231,6 +238,12 @@ tw_status tw_ctx_create(int device, size_t hbm_budget_bytes, tw_ctx **out)
     if (cudaMemPoolCreate(&c->pool, &pp) != cudaSuccess) return TW_ERR_CUDA;
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    const size_t ring = sizeof(tw::RJob) * tw_ctx::kJobSlots * tw_ctx::kJobsPerSlot;
+    if (cudaMallocHost((void **)&c->job_h, ring) != cudaSuccess) return destroy_partial(c.release());
+    if (cudaMalloc((void **)&c->job_d, ring) != cudaSuccess) return destroy_partial(c.release());
+    for (int s = 0; s < tw_ctx::kJobSlots; ++s)
+        if (cudaEventCreateWithFlags(&c->job_ev[s], cudaEventDisableTiming) != cudaSuccess)
+            return destroy_partial(c.release());
     *out = c.release();
     return TW_OK;
 }
@@ -246,6 +259,10 @@ tw_status tw_ctx_destroy(tw_ctx *ctx)
     if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
     if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    for (int s = 0; s < tw_ctx::kJobSlots; ++s)
+        if (ctx->job_ev[s]) cudaEventDestroy(ctx->job_ev[s]);
+    if (ctx->job_d) cudaFree(ctx->job_d);
+    if (ctx->job_h) cudaFreeHost(ctx->job_h);
     delete ctx;
     return TW_OK;
 }

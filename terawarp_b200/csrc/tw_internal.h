@@ -113,6 +113,17 @@ struct tw_ctx {
     cudaStream_t h2d = nullptr;         // host -> device copies
     cudaStream_t d2h = nullptr;         // device -> host copies
     cudaMemPool_t pool = nullptr;       // stream-ordered pool that keeps freed blocks
+    // Job descriptors of resample launches: a ring of slots, each a pinned
+    // host staging area with its device copy.  A slot is reused once the
+    // launch that last read it has completed (its event), so a launch of up
+    // to kJobsPerSlot jobs needs no allocation and no host wait.
+    static constexpr int kJobSlots = 8;
+    static constexpr int kJobsPerSlot = 64;
+    std::mutex job_mu;
+    tw::RJob *job_h = nullptr;          // pinned, kJobSlots x kJobsPerSlot
+    tw::RJob *job_d = nullptr;          // device, same shape
+    cudaEvent_t job_ev[kJobSlots] = {};
+    int job_next = 0;
     std::atomic<uint64_t> launches{0};
     mutable std::mutex err_mu;
     std::string last_error;

@@ -88,8 +88,26 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
         count(zs);
     }
     if (total == 0) return TW_OK;
-    RJob *d_jobs = nullptr;
     const size_t bytes = sizeof(RJob) * (size_t)njobs;
+    if (njobs <= tw_ctx::kJobsPerSlot && ctx->job_d) {
+        // descriptors through the context's slot ring: an asynchronous copy
+        // from pinned memory, so the host never waits for earlier work here
+        std::lock_guard<std::mutex> lk(ctx->job_mu);
+        const int s = ctx->job_next;
+        ctx->job_next = (s + 1) % tw_ctx::kJobSlots;
+        TW_CUDA_TRY(cudaEventSynchronize(ctx->job_ev[s]));  // the slot's previous launch has finished
+        RJob *h = ctx->job_h + (size_t)s * tw_ctx::kJobsPerSlot;
+        RJob *d = ctx->job_d + (size_t)s * tw_ctx::kJobsPerSlot;
+        std::memcpy(h, jobs, bytes);
+        TW_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+        cudaError_t e = launch_resample(d, njobs, total, jobs[0].dtype, jobs[0].kind, jobs[0].g, jobs[0].interp, st,
+                                        ctx->sm_count);
+        if (e != cudaSuccess) return fail(ctx, TW_ERR_CUDA, std::string("resample launch: ") + cudaGetErrorString(e));
+        TW_CUDA_TRY(cudaEventRecord(ctx->job_ev[s], st));
+        count_launch(ctx);
+        return TW_OK;
+    }
+    RJob *d_jobs = nullptr;
     TW_CUDA_TRY(cudaMallocAsync((void **)&d_jobs, bytes, st));
     TW_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs, bytes, cudaMemcpyHostToDevice, st));
     cudaError_t e = launch_resample(d_jobs, njobs, total, jobs[0].dtype, jobs[0].kind, jobs[0].g, jobs[0].interp, st,
