@@ -88,10 +88,10 @@ def _sz3(x) -> "C.Array":
 
 def _markers(pts) -> "C.Array":
     a = np.ascontiguousarray(np.asarray(pts, dtype=np.float32).reshape(-1, 3))
-    arr = (L.tw_marker * max(len(a), 1))()
-    for i, (x, y, z) in enumerate(a):
-        arr[i].x, arr[i].y, arr[i].z = float(x), float(y), float(z)
-    return arr
+    if len(a) == 0:
+        return (L.tw_marker * 1)()
+    # tw_marker is three packed floats, the same bytes as an (n, 3) float32 array
+    return (L.tw_marker * len(a)).from_buffer_copy(a.tobytes())
 
 
 def _like(x, shape):

@@ -57,6 +57,50 @@ void dfree(tw_ctx *ctx, void *p, size_t bytes)
     ctx->used.fetch_sub(bytes);
 }
 
+tw_status dmalloc_on(tw_ctx *ctx, void **p, size_t bytes, cudaStream_t st)
+{
+    *p = nullptr;
+    if (bytes == 0) return TW_OK;
+    size_t prev = ctx->used.fetch_add(bytes);
+    if (prev + bytes > ctx->budget) {
+        ctx->used.fetch_sub(bytes);
+        return fail(ctx, TW_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget");
+    }
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, st);
+    if (e != cudaSuccess) {
+        ctx->used.fetch_sub(bytes);
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(ctx, TW_ERR_OOM, std::string("device allocation: ") + cudaGetErrorString(e));
+    }
+    return TW_OK;
+}
+
+void dfree_on(tw_ctx *ctx, void *p, size_t bytes, cudaStream_t st)
+{
+    if (!p) return;
+    cudaFreeAsync(p, st);
+    ctx->used.fetch_sub(bytes);
+}
+
+tw_status upload(tw_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st)
+{
+    if (bytes == 0) return TW_OK;
+    if (bytes > tw_ctx::kStageBytes || !ctx->stage_h) {
+        TW_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        return TW_OK;
+    }
+    std::lock_guard<std::mutex> lk(ctx->stage_mu);
+    const int s = ctx->stage_next;
+    ctx->stage_next = (s + 1) % tw_ctx::kStageSlots;
+    TW_CUDA_TRY(cudaEventSynchronize(ctx->stage_ev[s]));  // the slot's previous copy has finished
+    unsigned char *h = ctx->stage_h + (size_t)s * tw_ctx::kStageBytes;
+    std::memcpy(h, src, bytes);
+    TW_CUDA_TRY(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, st));
+    TW_CUDA_TRY(cudaEventRecord(ctx->stage_ev[s], st));
+    return TW_OK;
+}
+
 int64_t grid_size(int64_t sz, int g) { return (int64_t)std::ceil((double)sz / (double)g) + 3; }
 
 bool is_device_ptr(const void *p)
@@ -100,34 +144,22 @@ tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *value
         o[0] += cx; o[1] += cy; o[2] += cz;
     }
     for (int a = 0; a < 3; ++a) o[a] = std::floor(o[a] / n + 0.5);
-    size_t cbytes = sizeof(double) * 4 * (size_t)n;
-    TW_TRY(dmalloc(ctx, (void **)&t->d_c, cbytes));
-    tw_status s = solve_tps_device(ctx, hc.data(), hv.data(), n, lambda, t->d_c, t->h_d, st);
+    // coefficients and the FP32 evaluation arrays (centres relative to o,
+    // negated coefficients) are all written on `st` by the solve, which waits
+    // for `st` once at its end; after that every stream may use them
+    const size_t cbytes = sizeof(double) * 4 * (size_t)n;
+    const size_t fbytes = sizeof(float4) * (size_t)n;
+    tw_status s = dmalloc_on(ctx, (void **)&t->d_c, cbytes, st);
+    if (s == TW_OK) s = dmalloc_on(ctx, (void **)&t->d_ctr32, fbytes, st);
+    if (s == TW_OK) s = dmalloc_on(ctx, (void **)&t->d_coef32, fbytes, st);
+    if (s == TW_OK)
+        s = solve_tps_device(ctx, hc.data(), hv.data(), n, lambda, t->d_c, t->h_d, o, t->d_ctr32, t->d_coef32, st);
     if (s != TW_OK) {
-        dfree(ctx, t->d_c, cbytes);
-        t->d_c = nullptr;
+        dfree_on(ctx, t->d_c, cbytes, st);
+        dfree_on(ctx, t->d_ctr32, fbytes, st);
+        dfree_on(ctx, t->d_coef32, fbytes, st);
         return s;
     }
-    // FP32 evaluation arrays: centres relative to o, negated coefficients
-    std::vector<double> hcoef(4 * (size_t)n);
-    TW_CUDA_TRY(cudaMemcpyAsync(hcoef.data(), t->d_c, cbytes, cudaMemcpyDeviceToHost, st));
-    TW_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<float4> c32(n), k32(n);
-    for (int i = 0; i < n; ++i) {
-        c32[i] = make_float4((float)(hc[3 * i] - o[0]), (float)(hc[3 * i + 1] - o[1]), (float)(hc[3 * i + 2] - o[2]), 0.f);
-        k32[i] = make_float4((float)(-hcoef[4 * i + 1]), (float)(-hcoef[4 * i + 2]), (float)(-hcoef[4 * i + 3]), 0.f);
-    }
-    size_t fbytes = sizeof(float4) * (size_t)n;
-    tw_status s2 = dmalloc(ctx, (void **)&t->d_ctr32, fbytes);
-    if (s2 == TW_OK) s2 = dmalloc(ctx, (void **)&t->d_coef32, fbytes);
-    if (s2 != TW_OK) {
-        dfree(ctx, t->d_c, cbytes);
-        dfree(ctx, t->d_ctr32, fbytes);
-        return s2;
-    }
-    TW_CUDA_TRY(cudaMemcpyAsync(t->d_ctr32, c32.data(), fbytes, cudaMemcpyHostToDevice, st));
-    TW_CUDA_TRY(cudaMemcpyAsync(t->d_coef32, k32.data(), fbytes, cudaMemcpyHostToDevice, st));
-    TW_CUDA_TRY(cudaStreamSynchronize(st));
     for (int a = 0; a < 3; ++a) t->o32[a] = o[a];
     t->h_ctr = new double[3 * (size_t)n];
     std::memcpy(t->h_ctr, hc.data(), sizeof(double) * 3 * n);
@@ -244,6 +276,11 @@ tw_status tw_ctx_create(int device, size_t hbm_budget_bytes, tw_ctx **out)
     for (int s = 0; s < tw_ctx::kJobSlots; ++s)
         if (cudaEventCreateWithFlags(&c->job_ev[s], cudaEventDisableTiming) != cudaSuccess)
             return destroy_partial(c.release());
+    if (cudaMallocHost((void **)&c->stage_h, tw_ctx::kStageBytes * tw_ctx::kStageSlots) != cudaSuccess)
+        return destroy_partial(c.release());
+    for (int s = 0; s < tw_ctx::kStageSlots; ++s)
+        if (cudaEventCreateWithFlags(&c->stage_ev[s], cudaEventDisableTiming) != cudaSuccess)
+            return destroy_partial(c.release());
     *out = c.release();
     return TW_OK;
 }
@@ -263,6 +300,9 @@ tw_status tw_ctx_destroy(tw_ctx *ctx)
         if (ctx->job_ev[s]) cudaEventDestroy(ctx->job_ev[s]);
     if (ctx->job_d) cudaFree(ctx->job_d);
     if (ctx->job_h) cudaFreeHost(ctx->job_h);
+    for (int s = 0; s < tw_ctx::kStageSlots; ++s)
+        if (ctx->stage_ev[s]) cudaEventDestroy(ctx->stage_ev[s]);
+    if (ctx->stage_h) cudaFreeHost(ctx->stage_h);
     delete ctx;
     return TW_OK;
 }

@@ -85,9 +85,12 @@ cudaError_t launch_tps_eval(const EvalParams &p, cudaStream_t st, int sm_count);
 // ------------------------------------------------------------------- solve
 
 struct SolveWork;   // device workspace of one solve
+// Solves on `st` and waits for it once, at the end.  When ctr32_out and
+// coef32_out are given it also writes the FP32 evaluation arrays: centres
+// relative to `o` and the negated non-affine coefficients (-c_x, -c_y, -c_z).
 tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
                            double *d_c_out /*n x 4 device*/, double *h_d_out /*4x4 host*/,
-                           cudaStream_t st);
+                           const double o[3], float4 *ctr32_out, float4 *coef32_out, cudaStream_t st);
 tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_sub, int n, double M[16],
                             cudaStream_t st);
 // The affine fit kernel alone on caller-provided device buffers (d_status
@@ -124,6 +127,13 @@ struct tw_ctx {
     tw::RJob *job_d = nullptr;          // device, same shape
     cudaEvent_t job_ev[kJobSlots] = {};
     int job_next = 0;
+    // pinned staging ring for small host -> device uploads (landmarks, ...)
+    static constexpr int kStageSlots = 8;
+    static constexpr size_t kStageBytes = (size_t)1 << 20;
+    std::mutex stage_mu;
+    unsigned char *stage_h = nullptr;   // pinned, kStageSlots x kStageBytes
+    cudaEvent_t stage_ev[kStageSlots] = {};
+    int stage_next = 0;
     std::atomic<uint64_t> launches{0};
     mutable std::mutex err_mu;
     std::string last_error;
@@ -145,5 +155,14 @@ tw_status fail(const tw_ctx *ctx, tw_status code, const std::string &msg);
 // Budgeted device allocation.
 tw_status dmalloc(tw_ctx *ctx, void **p, size_t bytes);
 void dfree(tw_ctx *ctx, void *p, size_t bytes);
+// Budgeted stream-ordered allocation on `st`, without a host wait: valid for
+// work queued on `st` after it, and for other streams only once the host has
+// waited for `st`.  dfree_on returns the block on `st`.
+tw_status dmalloc_on(tw_ctx *ctx, void **p, size_t bytes, cudaStream_t st);
+void dfree_on(tw_ctx *ctx, void *p, size_t bytes, cudaStream_t st);
+// Host -> device copy on `st` through the context's pinned staging ring, so
+// the host does not wait for earlier work on `st` (a pageable copy would);
+// copies larger than a staging slot fall back to a pageable copy.
+tw_status upload(tw_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st);
 inline void count_launch(tw_ctx *ctx, uint64_t k = 1) { if (ctx) ctx->launches += k; }
 }  // namespace tw

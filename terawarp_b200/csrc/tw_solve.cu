@@ -23,7 +23,9 @@
 //      to the polynomials), so it is factored by a blocked right-looking
 //      Cholesky: diagonal block in shared memory, panel TRSM, trailing SYRK
 //      in 64 x 64 FP64 tiles.
-//   4. z = Q' Y; w = A^-1 z(4:) by forward/back substitution;
+//   4. z = Q' Y; w = A^-1 z(4:): the forward substitution rides along in the
+//      factorisation (z(4:)' is an extra row block of the panel solves and
+//      trailing updates), the back substitution is one CTA;
 //      c = Q [0; w]; d = R^-1 (Q' (Y - K c))(0:4).
 //
 // Affine (reference: q_affine_compute_affinmatrix_3D,
@@ -194,13 +196,32 @@ __global__ void k_wvec(int n, const double *V, const double *tau, const double *
     }
 }
 
-// 3a. A (m x m, row-major) = (Q'KQ)(4:,4:) + lambda I
-__global__ void k_fill_a(const double *ctr, int n, const double *V, const double *W, double lambda, double *A)
+// The factorisation works on an (m + 4) x m row-major array: rows 0..m-1
+// hold A, rows m..m+3 hold the four right-hand sides z(4:) transposed.  Row
+// block ib < nblk covers rows 64 ib.., the extra row block nblk covers the
+// four right-hand-side rows.  The right-looking Cholesky treats that block like
+// any other row below the diagonal, so its panel solves and trailing updates
+// perform the forward substitution y = L^-1 z(4:) as part of the
+// factorisation, in parallel with it; rows m..m+3 end up holding y'.
+__device__ __forceinline__ int row_block_start(int ib, int nblk, int m) { return ib < nblk ? ib * kNB : m; }
+__device__ __forceinline__ int row_block_rows(int ib, int nblk, int m)
+{
+    return ib < nblk ? min(kNB, m - ib * kNB) : 4;
+}
+
+// 3a. A = (Q'KQ)(4:,4:) + lambda I, and the right-hand-side rows z(4:)'
+__global__ void k_fill_a(const double *__restrict__ ctr, int n, const double *__restrict__ V,
+                         const double *__restrict__ W, const double *__restrict__ Z, double lambda,
+                         double *__restrict__ A)
 {
     const int m = n - 4;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= m || j >= m) return;
+    if (i >= m + 4 || j >= m) return;
+    if (i >= m) {
+        A[(size_t)i * m + j] = Z[(j + 4) * 4 + (i - m)];
+        return;
+    }
     const int gi = i + 4, gj = j + 4;
     double v = kdist(ctr, gi, gj);
 #pragma unroll
@@ -209,66 +230,173 @@ __global__ void k_fill_a(const double *ctr, int n, const double *V, const double
     A[(size_t)i * m + j] = v;
 }
 
-// 3b. factor the diagonal block kb in shared memory
-__global__ void k_potrf(double *A, int m, int kb, int *status)
+// ---- 3b-4b: one cooperative kernel, one CTA of 256 threads per SM.
+//
+// The blocked right-looking Cholesky runs as phases separated by grid-wide
+// barriers: for each column block kb, CTA 0 factors the diagonal block
+// (potrf), every CTA takes row blocks of the panel (trsm), every CTA takes
+// 64 x 64 tiles of the trailing update (syrk).  The back substitution then
+// alternates CTA 0 solving a diagonal block with every CTA updating the rows
+// above it.  A phase is short (tens of microseconds), so a barrier instead
+// of a kernel launch per phase removes ~200 launches per solve.  L1 is not
+// coherent across SMs within a kernel, so every load of data another CTA may
+// have written in an earlier phase (A, z) bypasses L1 (__ldcg).
+
+constexpr int kSolveThreads = 256;
+constexpr int kStTimeout = 4;
+// a CTA gives up on a barrier after this long (ns); the launch is cooperative
+// so every CTA is resident, and the wait is bounded all the same
+constexpr unsigned long long kBarrierLimitNs = 5000000000ull;
+
+struct GridBar {
+    unsigned int count;   // CTAs arrived at the current barrier
+    unsigned int gen;     // barriers completed
+    int err;              // set by a CTA that gave up waiting
+    int pad;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
 {
-    __shared__ double a[kNB][kNB + 1];
-    const int r0 = kb * kNB;
-    const int nb = min(kNB, m - r0);
-    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-        int r = e / kNB, c = e % kNB;
-        a[r][c] = (r < nb && c < nb) ? A[(size_t)(r0 + r) * m + r0 + c] : (r == c ? 1.0 : 0.0);
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier with a bounded wait.  `gen` is the caller's count of
+// barriers passed (kept by thread 0).  Returns false, on every thread of the
+// CTA, if this or another CTA gave up; the caller then returns.
+__device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status)
+{
+    __shared__ int ok_sh;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned int g = gen;
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) + 1u == gridDim.x) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicExch(&b->gen, g + 1u);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            while (*reinterpret_cast<volatile unsigned int *>(&b->gen) == g) {
+                if (*reinterpret_cast<volatile int *>(&b->err) ||
+                    globaltimer_ns() - t0 > kBarrierLimitNs) {
+                    atomicOr(&b->err, 1);
+                    atomicOr(status, kStTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        gen = g + 1u;
+        if (*reinterpret_cast<volatile int *>(&b->err)) ok = 0;
+        ok_sh = ok;
     }
     __syncthreads();
+    return ok_sh != 0;
+}
+
+// potrf of diagonal block kb in shared memory: in step j threads j..63 take
+// the pivot (x rsqrt(d)) and scale column j, then each thread updates its 4 x 4
+// patch of the trailing lower triangle from register copies of the column.
+__device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, double *sm)
+{
+    double(*a)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double *sd = sm + kNB * (kNB + 1);
+    const int r0 = kb * kNB;
+    const int nb = min(kNB, m - r0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int r = e / kNB, c = e % kNB;
+        a[r][c] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int tr = (t >> 4) * 4, tc = (t & 15) * 4;
     for (int j = 0; j < kNB; ++j) {
-        if (threadIdx.x == 0) {
+        if (t >= j && t < kNB) {
             double d = a[j][j];
             if (!(d > 0.0)) {
-                atomicOr(status, kStNotSPD);
+                if (t == j) atomicOr(status, kStNotSPD);
                 d = 1.0;
             }
-            a[j][j] = sqrt(d);
+            const double inv = rsqrt(d);
+            if (t == j) sd[j] = d * inv;
+            else a[t][j] *= inv;
         }
         __syncthreads();
-        const double djj = a[j][j];
-        for (int i = j + 1 + threadIdx.x; i < kNB; i += blockDim.x) a[i][j] /= djj;
-        __syncthreads();
-        for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-            int i = e / kNB, l = e % kNB;
-            if (l > j && i >= l) a[i][l] -= a[i][j] * a[l][j];
+        if (tr + 3 > j) {
+            double ci[4], cl[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                ci[u] = a[tr + u][j];
+                cl[u] = a[tc + u][j];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int i = tr + u, l = tc + v;
+                    if (l > j && i >= l) a[i][l] -= ci[u] * cl[v];
+                }
         }
         __syncthreads();
     }
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
-        if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c <= r ? a[r][c] : 0.0;
+        if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c < r ? a[r][c] : (c == r ? sd[r] : 0.0);
     }
 }
 
-// 3c. panel: L(ib,kb) = A(ib,kb) L(kb,kb)^-T for all ib > kb; one CTA per
-// row block, one thread per row.
-__global__ void k_trsm(double *A, int m, int kb)
+// trsm of row block ib against diagonal block kb: L(ib,kb) = A(ib,kb) L(kb,kb)^-T.
+// Thread (r, q) keeps row r's columns q, q+4, .. in registers; column c is
+// finished by its owner (x 1/L(c,c)), broadcast through shared memory, and
+// subtracted from the later columns: X(r,c') -= X(r,c) L(c',c).
+__device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double *sm)
 {
-    extern __shared__ double dsm[];
-    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm);
-    double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm + kNB * (kNB + 1));
+    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
+    double(*xs)[kNB] = reinterpret_cast<double(*)[kNB]>(sm + 2 * kNB * (kNB + 1));
+    double *rdiag = sm + 2 * kNB * (kNB + 1) + 2 * kNB;
+    const int nblk = (m + kNB - 1) / kNB;
     const int r0 = kb * kNB;
-    const int ib = kb + 1 + blockIdx.x;
-    const int i0 = ib * kNB;
+    const int i0 = row_block_start(ib, nblk, m);
     const int nbk = min(kNB, m - r0);
-    const int nbi = min(kNB, m - i0);
+    const int nbi = row_block_rows(ib, nblk, m);
+    __syncthreads();
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
-        L[r][c] = (r < nbk && c < nbk) ? A[(size_t)(r0 + r) * m + r0 + c] : (r == c ? 1.0 : 0.0);
-        X[r][c] = (r < nbi && c < nbk) ? A[(size_t)(i0 + r) * m + r0 + c] : 0.0;
+        L[r][c] = (r < nbk && c < nbk) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
+        X[r][c] = (r < nbi && c < nbk) ? __ldcg(&A[(size_t)(i0 + r) * m + r0 + c]) : 0.0;
     }
     __syncthreads();
-    const int r = threadIdx.x;
-    if (r < nbi) {
-        for (int c = 0; c < nbk; ++c) {
-            double s = X[r][c];
-            for (int p = 0; p < c; ++p) s -= X[r][p] * L[c][p];
-            X[r][c] = s / L[c][c];
+    if (threadIdx.x < kNB) rdiag[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
+    const int r = threadIdx.x & (kNB - 1);
+    const int q = threadIdx.x >> 6;
+    double x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = X[r][4 * k + q];
+    __syncthreads();  // X is rewritten below as columns finish
+    // fully unrolled so that every index into x is a constant (x stays in
+    // registers); columns at or beyond nbk are skipped
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) {
+        if (c >= nbk) break;
+        if (q == (c & 3)) {
+            // the finished column goes straight to X (it is not updated again)
+            const double own = x[c >> 2] * rdiag[c];
+            X[r][c] = own;
+            xs[c & 1][r] = own;
+        }
+        __syncthreads();
+        const double xc = xs[c & 1][r];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int cp = 4 * k + q;
+            if (cp > c && cp < nbk) x[k] -= xc * L[cp][c];
         }
     }
     __syncthreads();
@@ -278,27 +406,28 @@ __global__ void k_trsm(double *A, int m, int kb)
     }
 }
 
-// 3d. trailing update A(ib,jb) -= L(ib,kb) L(jb,kb)' for kb < jb <= ib.
-// blockIdx.x enumerates the lower-triangular block pairs of the trailing
-// matrix; 256 threads, each owning a 4 x 4 patch of the 64 x 64 tile.
-__global__ void __launch_bounds__(256) k_syrk(double *A, int m, int kb)
+// syrk tile number t of step kb: A(ib,jb) -= L(ib,kb) L(jb,kb)' for
+// kb < jb <= ib, jb a column block and ib a row block (the right-hand-side
+// block included), t enumerating the pairs; each thread owns a 4 x 4 patch.
+__device__ void syrk_tile(double *__restrict__ A, int m, int kb, long long t, double *sm)
 {
-    extern __shared__ double dsm[];
-    double(*Li)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm);
-    double(*Lj)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(dsm + kNB * (kNB + 1));
+    double(*Li)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double(*Lj)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
+    const int nblk = (m + kNB - 1) / kNB;
     // invert t = ib'(ib'+1)/2 + jb' (0 <= jb' <= ib')
-    const long long t = blockIdx.x;
     int ibp = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
     while ((long long)(ibp + 1) * (ibp + 2) / 2 <= t) ++ibp;
     while ((long long)ibp * (ibp + 1) / 2 > t) --ibp;
     const int jbp = (int)(t - (long long)ibp * (ibp + 1) / 2);
     const int ib = kb + 1 + ibp, jb = kb + 1 + jbp;
-    const int r0 = kb * kNB, i0 = ib * kNB, j0 = jb * kNB;
-    const int nbk = min(kNB, m - r0), nbi = min(kNB, m - i0), nbj = min(kNB, m - j0);
+    if (jb >= nblk) return;  // the right-hand-side block has no diagonal tile
+    const int r0 = kb * kNB, i0 = row_block_start(ib, nblk, m), j0 = jb * kNB;
+    const int nbk = min(kNB, m - r0), nbi = row_block_rows(ib, nblk, m), nbj = min(kNB, m - j0);
+    __syncthreads();
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
-        Li[r][c] = (r < nbi && c < nbk) ? A[(size_t)(i0 + r) * m + r0 + c] : 0.0;
-        Lj[r][c] = (r < nbj && c < nbk) ? A[(size_t)(j0 + r) * m + r0 + c] : 0.0;
+        Li[r][c] = (r < nbi && c < nbk) ? __ldcg(&A[(size_t)(i0 + r) * m + r0 + c]) : 0.0;
+        Lj[r][c] = (r < nbj && c < nbk) ? __ldcg(&A[(size_t)(j0 + r) * m + r0 + c]) : 0.0;
     }
     __syncthreads();
     const int tr = (threadIdx.x / 16) * 4, tc = (threadIdx.x % 16) * 4;
@@ -320,76 +449,89 @@ __global__ void __launch_bounds__(256) k_syrk(double *A, int m, int kb)
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             int r = tr + u, c = tc + v;
-            if (r < nbi && c < nbj && (ib != jb || c <= r)) A[(size_t)(i0 + r) * m + j0 + c] -= acc[u][v];
+            if (r < nbi && c < nbj && (ib != jb || c <= r)) {
+                double *dst = &A[(size_t)(i0 + r) * m + j0 + c];
+                *dst = __ldcg(dst) - acc[u][v];
+            }
         }
 }
 
-// 4a. forward substitution L y = z(4:) for 4 right-hand sides, in place in
-// Z rows 4..n-1.  One CTA of 1024 threads.
-__global__ void k_fwd(const double *A, int m, double *Z)
+// Back substitution, diagonal block kb (CTA 0): solve D' x = z(block) for the
+// four right-hand sides; warp c takes right-hand side c, lane l rows l and
+// l + 32; row j of D is column j of D'.  x overwrites z(block).
+__device__ void bwd_diag(const double *__restrict__ A, int m, int kb, double *__restrict__ z, double *sm)
 {
-    __shared__ double y[kNB][4];
-    double *z = Z + 16;  // rows 4.. of the n x 4 Z
-    for (int kb = 0; kb * kNB < m; ++kb) {
-        const int r0 = kb * kNB, nb = min(kNB, m - r0);
-        // diagonal block: warp c handles right-hand side c
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (warp < 4) {
-            for (int r = 0; r < nb; ++r) {
-                double s = 0.0;
-                for (int p = lane; p < r; p += 32) s += A[(size_t)(r0 + r) * m + r0 + p] * y[p][warp];
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) y[r][warp] = (z[(r0 + r) * 4 + warp] - s) / A[(size_t)(r0 + r) * m + r0 + r];
-                __syncwarp();
+    double(*D)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double *dinv = sm + kNB * (kNB + 1);
+    const int r0 = kb * kNB, nb = min(kNB, m - r0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        const int r = e / kNB, c = e % kNB;
+        D[r][c] = (r < nb && c <= r) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : 0.0;
+    }
+    if (threadIdx.x < nb) dinv[threadIdx.x] = 1.0 / __ldcg(&A[(size_t)(r0 + threadIdx.x) * m + r0 + threadIdx.x]);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 4) {
+        double b0 = lane < nb ? __ldcg(&z[(r0 + lane) * 4 + warp]) : 0.0;
+        double b1 = lane + 32 < nb ? __ldcg(&z[(r0 + lane + 32) * 4 + warp]) : 0.0;
+        for (int j = nb - 1; j >= 0; --j) {
+            const double bj = __shfl_sync(0xffffffffu, j < 32 ? b0 : b1, j & 31);
+            const double xj = bj * dinv[j];
+            if (lane == (j & 31)) {
+                if (j < 32) b0 = xj;
+                else b1 = xj;
             }
+            if (lane < j) b0 -= D[j][lane] * xj;
+            if (lane + 32 < j) b1 -= D[j][lane + 32] * xj;
         }
-        __syncthreads();
-        for (int r = threadIdx.x; r < nb * 4; r += blockDim.x) z[(r0 + r / 4) * 4 + (r % 4)] = y[r / 4][r % 4];
-        // update the rows below
-        for (int i = r0 + nb + threadIdx.x; i < m; i += blockDim.x) {
-            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-            const double *Li = A + (size_t)i * m + r0;
-            for (int p = 0; p < nb; ++p) {
-                const double l = Li[p];
-                s0 += l * y[p][0]; s1 += l * y[p][1]; s2 += l * y[p][2]; s3 += l * y[p][3];
-            }
-            z[i * 4 + 0] -= s0; z[i * 4 + 1] -= s1; z[i * 4 + 2] -= s2; z[i * 4 + 3] -= s3;
-        }
-        __syncthreads();
+        if (lane < nb) z[(r0 + lane) * 4 + warp] = b0;
+        if (lane + 32 < nb) z[(r0 + lane + 32) * 4 + warp] = b1;
     }
 }
 
-// 4b. back substitution L' x = y, in place.
-__global__ void k_bwd(const double *A, int m, double *Z)
+__global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict__ A, int m, double *__restrict__ Z,
+                                                              int *status, GridBar *bar)
 {
-    __shared__ double x[kNB][4];
-    double *z = Z + 16;
+    extern __shared__ double sm[];
+    unsigned int gen = 0;
     const int nblk = (m + kNB - 1) / kNB;
+    for (int kb = 0; kb < nblk; ++kb) {
+        if (blockIdx.x == 0) potrf_tile(A, m, kb, status, sm);
+        if (!grid_sync(bar, gen, status)) return;
+        const int rest = nblk - kb - 1;
+        // row blocks below the diagonal: the rest of A plus the right-hand-side block
+        for (int b = blockIdx.x; b < rest + 1; b += gridDim.x) trsm_tile(A, m, kb, kb + 1 + b, sm);
+        if (!grid_sync(bar, gen, status)) return;
+        const long long pairs = (long long)(rest + 1) * (rest + 2) / 2;
+        for (long long t = blockIdx.x; t < pairs; t += gridDim.x) syrk_tile(A, m, kb, t, sm);
+        if (!grid_sync(bar, gen, status)) return;
+    }
+    // y' sits in rows m..m+3; back substitution L' x = y into Z rows 4..n-1
+    double *z = Z + 16;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    for (int e = gt; e < 4 * m; e += gstride) z[e] = __ldcg(&A[(size_t)(m + (e & 3)) * m + (e >> 2)]);
+    if (!grid_sync(bar, gen, status)) return;
     for (int kb = nblk - 1; kb >= 0; --kb) {
+        if (blockIdx.x == 0) bwd_diag(A, m, kb, z, sm);
+        if (!grid_sync(bar, gen, status)) return;
         const int r0 = kb * kNB, nb = min(kNB, m - r0);
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (warp < 4) {
-            for (int r = nb - 1; r >= 0; --r) {
-                double s = 0.0;
-                for (int p = r + 1 + lane; p < nb; p += 32) s += A[(size_t)(r0 + p) * m + r0 + r] * x[p][warp];
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) x[r][warp] = (z[(r0 + r) * 4 + warp] - s) / A[(size_t)(r0 + r) * m + r0 + r];
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        for (int r = threadIdx.x; r < nb * 4; r += blockDim.x) z[(r0 + r / 4) * 4 + (r % 4)] = x[r / 4][r % 4];
-        for (int i = threadIdx.x; i < r0; i += blockDim.x) {
+        for (int i = gt; i < r0; i += gstride) {
             double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll 8
             for (int p = 0; p < nb; ++p) {
-                const double l = A[(size_t)(r0 + p) * m + i];
-                s0 += l * x[p][0]; s1 += l * x[p][1]; s2 += l * x[p][2]; s3 += l * x[p][3];
+                const double l = __ldcg(&A[(size_t)(r0 + p) * m + i]);
+                const double *xp = z + (r0 + p) * 4;
+                s0 += l * __ldcg(xp); s1 += l * __ldcg(xp + 1); s2 += l * __ldcg(xp + 2); s3 += l * __ldcg(xp + 3);
             }
-            z[i * 4 + 0] -= s0; z[i * 4 + 1] -= s1; z[i * 4 + 2] -= s2; z[i * 4 + 3] -= s3;
+            double *zi = z + i * 4;
+            zi[0] = __ldcg(zi) - s0; zi[1] = __ldcg(zi + 1) - s1; zi[2] = __ldcg(zi + 2) - s2; zi[3] = __ldcg(zi + 3) - s3;
         }
-        __syncthreads();
+        if (!grid_sync(bar, gen, status)) return;
     }
 }
+
+constexpr size_t kSolveSmem = sizeof(double) * (2 * kNB * (kNB + 1) + 3 * kNB);
 
 // 4c. c = H1 H2 H3 H4 [0; w]  (Z rows 0..3 are replaced by zeros)
 __global__ void k_apply_q(int n, const double *V, const double *tau, const double *Z, double *C)
@@ -434,6 +576,17 @@ __global__ void k_finish_d(int n, const double *V, const double *tau, const doub
                 d_out[a * 4 + c] = s / R[a * 4 + a];
             }
     }
+}
+
+// 5. FP32 evaluation arrays: centres relative to the origin o, and the
+// negated non-affine coefficients (-c_x, -c_y, -c_z, 0).
+__global__ void k_eval_arrays(int n, const double *ctr, const double *C, double ox, double oy, double oz,
+                              float4 *ctr32, float4 *coef32)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ctr32[i] = make_float4((float)(ctr[3 * i] - ox), (float)(ctr[3 * i + 1] - oy), (float)(ctr[3 * i + 2] - oz), 0.f);
+    coef32[i] = make_float4((float)(-C[4 * i + 1]), (float)(-C[4 * i + 2]), (float)(-C[4 * i + 3]), 0.f);
 }
 
 // ----------------------------------------------------------- affine DLT
@@ -553,17 +706,28 @@ struct DevBuf {
     ~DevBuf() { if (p) dfree(ctx, p, bytes); }
 };
 
+struct StreamBuf {
+    tw_ctx *ctx = nullptr;
+    cudaStream_t st = nullptr;
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~StreamBuf() { if (p) dfree_on(ctx, p, bytes, st); }
+};
+
 }  // namespace
 
 tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
-                           double *d_c_out, double *h_d_out, cudaStream_t st)
+                           double *d_c_out, double *h_d_out, const double o[3], float4 *ctr32_out,
+                           float4 *coef32_out, cudaStream_t st)
 {
     const int m = n - 4;
     // workspace: ctr 3n, Y 4n, Xw 4n, V 4n, P 4n, W 4n, Z 4n, KC 4n, tau 4, R 16, d 16, status
-    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + 16 + 2;
-    DevBuf ws{ctx}, abuf{ctx};
+    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + 16 + 2 + 2;
+    // stream-ordered workspace on `st`, returned to the pool on `st` when this
+    // function exits (after the final wait, or with the error)
+    StreamBuf ws{ctx, st}, abuf{ctx, st};
     ws.bytes = small * sizeof(double);
-    TW_TRY(dmalloc(ctx, &ws.p, ws.bytes));
+    TW_TRY(dmalloc_on(ctx, &ws.p, ws.bytes, st));
     double *base = static_cast<double *>(ws.p);
     double *d_ctr = base;
     double *d_Y = d_ctr + 3 * (size_t)n;
@@ -577,9 +741,10 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
     double *d_R = d_tau + 4;
     double *d_d = d_R + 16;
     int *d_status = reinterpret_cast<int *>(d_d + 16);
+    GridBar *d_bar = reinterpret_cast<GridBar *>(d_d + 18);  // 16 bytes, 8-byte aligned
     if (m > 0) {
-        abuf.bytes = (size_t)m * m * sizeof(double);
-        TW_TRY(dmalloc(ctx, &abuf.p, abuf.bytes));
+        abuf.bytes = (size_t)(m + 4) * m * sizeof(double);
+        TW_TRY(dmalloc_on(ctx, &abuf.p, abuf.bytes, st));
     }
     double *d_A = static_cast<double *>(abuf.p);
 
@@ -590,8 +755,8 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
         hY[4 * i + 2] = h_val[3 * i + 1];
         hY[4 * i + 3] = h_val[3 * i + 2];
     }
-    TW_CUDA_TRY(cudaMemcpyAsync(d_ctr, h_ctr, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
-    TW_CUDA_TRY(cudaMemcpyAsync(d_Y, hY.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice, st));
+    TW_TRY(upload(ctx, d_ctr, h_ctr, sizeof(double) * 3 * n, st));
+    TW_TRY(upload(ctx, d_Y, hY.data(), sizeof(double) * 4 * n, st));
     TW_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     TW_CUDA_TRY(cudaMemsetAsync(d_d, 0, sizeof(double) * 16, st));
 
@@ -604,32 +769,28 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
     k_wvec<<<1, kRedThreads, 0, st>>>(n, d_V, d_tau, d_P, d_W, d_Y, d_Z);
     nl += 2;
     if (m > 0) {
-        dim3 b(32, 8), g((m + 31) / 32, (m + 7) / 8);
-        k_fill_a<<<g, b, 0, st>>>(d_ctr, n, d_V, d_W, lambda, d_A);
+        dim3 b(32, 8), g((m + 31) / 32, (m + 4 + 7) / 8);
+        k_fill_a<<<g, b, 0, st>>>(d_ctr, n, d_V, d_W, d_Z, lambda, d_A);
         ++nl;
-        const int nblk = (m + kNB - 1) / kNB;
-        const int tile_smem = (int)(2 * sizeof(double) * kNB * (kNB + 1));
-        TW_CUDA_TRY(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
-        TW_CUDA_TRY(cudaFuncSetAttribute(k_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem));
-        for (int kb = 0; kb < nblk; ++kb) {
-            k_potrf<<<1, 256, 0, st>>>(d_A, m, kb, d_status);
-            ++nl;
-            const int rest = nblk - kb - 1;
-            if (rest > 0) {
-                k_trsm<<<rest, kNB, tile_smem, st>>>(d_A, m, kb);
-                const long long pairs = (long long)rest * (rest + 1) / 2;
-                k_syrk<<<(unsigned)pairs, 256, tile_smem, st>>>(d_A, m, kb);
-                nl += 2;
-            }
-        }
-        k_fwd<<<1, kRedThreads, 0, st>>>(d_A, m, d_Z);
-        k_bwd<<<1, kRedThreads, 0, st>>>(d_A, m, d_Z);
-        nl += 2;
+        TW_CUDA_TRY(cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem));
+        int per_sm = 0;
+        TW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_solve, kSolveThreads, kSolveSmem));
+        if (per_sm < 1) return fail(ctx, TW_ERR_CUDA, "solve kernel does not fit on an SM");
+        int grid = ctx->sm_count;
+        TW_CUDA_TRY(cudaMemsetAsync(d_bar, 0, sizeof(GridBar), st));
+        void *args[] = {(void *)&d_A, (void *)&m, (void *)&d_Z, (void *)&d_status, (void *)&d_bar};
+        TW_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_chol_solve, dim3(grid), dim3(kSolveThreads), args,
+                                                kSolveSmem, st));
+        ++nl;
     }
     k_apply_q<<<1, kRedThreads, 0, st>>>(n, d_V, d_tau, d_Z, d_c_out);
     k_kmul<<<kgrid, 32 * warps_per_block, 0, st>>>(d_ctr, n, d_c_out, d_KC);
     k_finish_d<<<1, kRedThreads, 0, st>>>(n, d_V, d_tau, d_R, d_Y, d_KC, d_d);
     nl += 3;
+    if (ctr32_out && coef32_out) {
+        k_eval_arrays<<<(n + 255) / 256, 256, 0, st>>>(n, d_ctr, d_c_out, o[0], o[1], o[2], ctr32_out, coef32_out);
+        ++nl;
+    }
     TW_CUDA_TRY(cudaGetLastError());
     count_launch(ctx, nl);
     int status = 0;
@@ -638,6 +799,8 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
     TW_CUDA_TRY(cudaStreamSynchronize(st));
     if (status & kStSingularX)
         return fail(ctx, TW_ERR_SINGULAR, "TPS centres are degenerate: [1 s] is rank deficient (coplanar or < 4 distinct points)");
+    if (status & kStTimeout)
+        return fail(ctx, TW_ERR_TIMEOUT, "TPS solve: a grid barrier timed out");
     if (status & kStNotSPD)
         return fail(ctx, TW_ERR_SINGULAR, "projected TPS system is not positive definite");
     return TW_OK;
