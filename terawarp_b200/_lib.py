@@ -107,15 +107,19 @@ def load() -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    if os.environ.get("TW_NO_BUILD") != "1":
+    path = LIB_PATH
+    override = os.environ.get("TW_LIBRARY")  # an alternative build of the same ABI
+    if override:
+        path = Path(override)
+    elif os.environ.get("TW_NO_BUILD") != "1":
         try:
             from . import build as _build
             _build.build()
         except FileNotFoundError:
             pass
-    if not LIB_PATH.exists():
-        raise RuntimeError(f"libterawarp_b200.so not found at {LIB_PATH}; run terawarp_b200.build.build()")
-    lib = C.CDLL(str(LIB_PATH))
+    if not path.exists():
+        raise RuntimeError(f"libterawarp_b200.so not found at {path}; run terawarp_b200.build.build()")
+    lib = C.CDLL(str(path))
     for name, (res, args) in SIGNATURES.items():
         f = getattr(lib, name)
         f.restype = res

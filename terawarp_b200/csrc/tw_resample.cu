@@ -36,6 +36,9 @@ namespace tw {
 namespace {
 
 constexpr int kThreads = 256;
+#ifndef TW_RES_MINB
+#define TW_RES_MINB 3  // resident CTAs per SM the TPS kernel is compiled for (register budget)
+#endif
 constexpr int kTX = 32;
 constexpr int kTY = 8;
 constexpr int kV = 8;                 // voxels per lane per brick row (4 pairs)
@@ -391,37 +394,57 @@ __device__ __forceinline__ void pair_positions(const float4 n[4], const PairW &p
 }
 
 // The four source rows a trilinear sample reads, (dy, dz) = (r & 1, r >> 1),
-// as base pointers of one brick, plus the int32 pitches: a tap address is
-// then one wide multiply-add of a 32-bit offset onto a row base.
+// as base pointers of one brick, plus the int32 pitches.  The bases sit at
+// the low corner of the brick's sample hull, so every unchecked tap is a
+// non-negative 32-bit element offset from them, and a tap address is one
+// wide unsigned multiply-add onto a row base.
 template <typename T>
 struct Rows {
     const T *rb[4];
     int py, pz;
-    uint32_t k;  // magic-number bias folded out of the offsets
+    uint32_t k;  // magic-number bias and the hull corner folded out of the offsets
 };
 
+// lo: the hull's low corner relative to `base` (used only when `valid`, i.e.
+// when the brick has unchecked samples and all its offsets fit int32).
 template <typename T>
-__device__ __forceinline__ Rows<T> make_rows(const T *base, int py, int pz)
+__device__ __forceinline__ Rows<T> make_rows(const T *base, int py, int pz, const float (&lo)[3], bool valid)
 {
+    // one voxel of slack below the hull: a sample computed in FP32 may fall a
+    // rounding error below the exact bound
+    int il[3] = {0, 0, 0};
+    if (valid)
+        for (int a = 0; a < 3; ++a) il[a] = (int)floorf(lo[a]) - 1;
+    const int omin = il[2] * pz + il[1] * py + il[0];
+    const T *b = base + omin;
     Rows<T> r;
-    r.rb[0] = base;
-    r.rb[1] = base + py;
-    r.rb[2] = base + pz;
-    r.rb[3] = base + pz + py;
+    r.rb[0] = b;
+    r.rb[1] = b + py;
+    r.rb[2] = b + pz;
+    r.rb[3] = b + pz + py;
     r.py = py;
     r.pz = pz;
-    r.k = (uint32_t)kMagicBits * (uint32_t)(pz + py + 1);
+    r.k = (uint32_t)kMagicBits * (uint32_t)(pz + py + 1) + (uint32_t)omin;
     return r;
 }
 
-// Element offset of floor(q) from the magic-floor bit patterns (2^32 wrap
-// arithmetic; the result is the exact offset because it fits int32).
+// Element offset of floor(q) from the rows' hull corner, from the
+// magic-floor bit patterns (2^32 wrap arithmetic; exact because the result
+// lies in [0, 2^31)).
 template <typename T>
-__device__ __forceinline__ int tap_offset(const Rows<T> &R, float mx, float my, float mz)
+__device__ __forceinline__ uint32_t tap_offset(const Rows<T> &R, float mx, float my, float mz)
 {
-    const uint32_t o = (uint32_t)__float_as_int(mz) * (uint32_t)R.pz + (uint32_t)__float_as_int(my) * (uint32_t)R.py +
-                       (uint32_t)__float_as_int(mx) - R.k;
-    return (int)o;
+    return (uint32_t)__float_as_int(mz) * (uint32_t)R.pz + (uint32_t)__float_as_int(my) * (uint32_t)R.py +
+           (uint32_t)__float_as_int(mx) - R.k;
+}
+
+// base + o elements as one wide unsigned multiply-add.
+template <typename T>
+__device__ __forceinline__ const T *wide_addr(const T *base, uint32_t o)
+{
+    const T *p;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(p) : "r"(o), "r"((uint32_t)sizeof(T)), "l"(base));
+    return p;
 }
 
 // Unchecked sample of a voxel pair at positions (p0, p1, pz2): every tap is
@@ -433,13 +456,13 @@ __device__ __forceinline__ void pair_fast2(float2 p0, float2 p1, float2 pz2, con
     // floor via add.rm of 1.5*2^23, fractions
     const float2 m0 = __fadd2_rd(p0, MM), m1 = __fadd2_rd(p1, MM), mz = __fadd2_rd(pz2, MM);
     const float2 f0 = sub2(p0, sub2(m0, MM)), f1 = sub2(p1, sub2(m1, MM)), fz = sub2(pz2, sub2(mz, MM));
-    const int off0 = tap_offset(R, m0.x, m0.y, mz.x);
-    const int off1 = tap_offset(R, m1.x, m1.y, mz.y);
+    const uint32_t off0 = tap_offset(R, m0.x, m0.y, mz.x);
+    const uint32_t off1 = tap_offset(R, m1.x, m1.y, mz.y);
     // magic floats of the 8 taps of both voxels
     float2 lo[4], hi[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const T *q0 = R.rb[r] + off0, *q1 = R.rb[r] + off1;
+        const T *q0 = wide_addr(R.rb[r], off0), *q1 = wide_addr(R.rb[r], off1);
         lo[r] = f2(mag(q0), mag(q1));
         hi[r] = f2(mag(q0 + 1), mag(q1 + 1));
     }
@@ -601,11 +624,12 @@ __device__ __forceinline__ void tps_pair(const float4 *Q, const BrickCtx<T> &B, 
     store_pair<T>(drow + x, outv[0], outv[1], B.pair_ok, fast ? 2 : B.xe - x);
 }
 
-// ALL_FAST: the whole brick is inside; else segf[y*4 + k] says whether the
-// warp-row segment (row y, voxels 64k..64k+63) may skip the bounds checks.
+// ALL_FAST: the whole slice is inside; else segf[y*4 + k] says whether the
+// warp-row segment (row y, voxels 64k..64k+63) may skip the bounds checks in
+// x and y, and z_fast whether the slice may in z.
 template <typename T, int G, int INTERP, bool ALL_FAST>
 __device__ __forceinline__ void tps_rows(const float4 *Q, const BrickCtx<T> &B, int lane, int ty, int ye, T *dslice,
-                                         int64_t dpy, const unsigned char *segf)
+                                         int64_t dpy, const unsigned char *segf, bool z_fast)
 {
     using Gm = Geom<G>;
 #pragma unroll 1
@@ -618,7 +642,7 @@ __device__ __forceinline__ void tps_rows(const float4 *Q, const BrickCtx<T> &B, 
             const int x = 2 * lane + 64 * k;
             if (ALL_FAST) {
                 tps_pair<T, G, INTERP>(Q, B, y, x, true, drow);
-            } else if (segf[y * 4 + k]) {  // warp-uniform
+            } else if (z_fast && segf[y * 4 + k]) {  // warp-uniform
                 tps_pair<T, G, INTERP>(Q, B, y, x, true, drow);
             } else if (x < B.xe) {
                 tps_pair<T, G, INTERP>(Q, B, y, x, false, drow);
@@ -650,9 +674,9 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     const int64_t c0[3] = {O[0] / G, O[1] / G, O[2] / G};  // first cell (= first node index)
     const int zoff = (int)(zfirst - O[2]);                 // first plane within the cell layer
 
-    // 1. stage node' = DF + node position - O, and its hull (a non-finite
-    // node forces the checked path)
-    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    // 1. stage node' = DF + node position - O, and the range of DF (a
+    // non-finite node forces the checked path)
+    float dmn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, dmx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
     for (int i = tid; i < Gm::ND; i += kThreads) {
         int nx = i % Gm::NX, t = i / Gm::NX;
         int ny = t % Gm::NY, nz = t / Gm::NY;
@@ -669,19 +693,27 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
         v.w = 0.f;
         Nd[i] = v;
         if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) {
-            mn[0] = fminf(mn[0], v.x); mn[1] = fminf(mn[1], v.y); mn[2] = fminf(mn[2], v.z);
-            mx[0] = fmaxf(mx[0], v.x); mx[1] = fmaxf(mx[1], v.y); mx[2] = fmaxf(mx[2], v.z);
+            dmn[0] = fminf(dmn[0], d.x); dmn[1] = fminf(dmn[1], d.y); dmn[2] = fminf(dmn[2], d.z);
+            dmx[0] = fmaxf(dmx[0], d.x); dmx[1] = fmaxf(dmx[1], d.y); dmx[2] = fmaxf(dmx[2], d.z);
         } else {
-            mn[0] = mn[1] = mn[2] = -3.4e38f;
-            mx[0] = mx[1] = mx[2] = 3.4e38f;
+            dmn[0] = dmn[1] = dmn[2] = -3.4e38f;
+            dmx[0] = dmx[1] = dmx[2] = 3.4e38f;
         }
     }
-    block_minmax(mn, mx, red);  // contains __syncthreads (Nd visible after it)
+    block_minmax(dmn, dmx, red);  // contains __syncthreads (Nd visible after it)
 
-    const bool inside_out = (O[0] + Gm::BX <= J.out_o[0] + J.out_n[0]) &&
-                            (O[1] + Gm::BY <= J.out_o[1] + J.out_n[1]) &&
-                            (zfirst + zs <= J.out_o[2] + J.out_n[2]);
-    const bool fast = inside_out && hull_inside(J, O, mn, mx);
+    // Sample hull.  The B-spline weights are >= 0 and sum to 1, and the spline
+    // reproduces the linear node positions, so a voxel at brick position p
+    // samples q = p + (a convex combination of DF): per axis q lies in
+    // [p + min DF, p + max DF].  This is far tighter than the hull of the
+    // staged nodes, whose outer ring lies a whole cell beyond the brick.
+    const float plo[3] = {0.f, 0.f, (float)zoff};
+    const float phi[3] = {(float)(Gm::BX - 1), (float)(Gm::BY - 1), (float)(zoff + zs - 1)};
+    float mn[3], mx[3];
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = dmn[a] <= -3.0e38f ? -3.4e38f : plo[a] + dmn[a];
+        mx[a] = dmx[a] >= 3.0e38f ? 3.4e38f : phi[a] + dmx[a];
+    }
     const Frame frame = make_frame(J, O);
     const bool span_ok = offsets_fit_32(J, mn, mx);
     const Clamp cw = make_clamp(J, frame, mn, mx);
@@ -701,34 +733,33 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
         r.w = 0.f;
         R[i] = r;
     }
-    __syncthreads();
 
-    // per row segment (row y, 64 voxels 64k..64k+63): does the hull of the
-    // y-contracted nodes it uses (all four z layers, weights >= 0) keep every
-    // tap inside the volume and the buffer?  Then that warp-row segment takes
-    // the unchecked path even in a border brick.
-    const int64_t xe = J.out_o[0] + J.out_n[0] - O[0];  // valid x extent in this brick
-    if (!fast && tid < Gm::BY * 4) {
-        const int y = tid >> 2, k = tid & 3;
-        const int t0 = (64 * k) / G, t1 = (64 * k + 63) / G + 3;
-        float lo3[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi3[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
-        bool finite = true;
-        for (int c = 0; c < 4; ++c)
-            for (int nx = t0; nx <= t1; ++nx) {
-                const float4 r = R[(y * 4 + c) * Gm::NX + nx];
-                finite = finite && isfinite(r.x) && isfinite(r.y) && isfinite(r.z);
-                lo3[0] = fminf(lo3[0], r.x); lo3[1] = fminf(lo3[1], r.y); lo3[2] = fminf(lo3[2], r.z);
-                hi3[0] = fmaxf(hi3[0], r.x); hi3[1] = fmaxf(hi3[1], r.y); hi3[2] = fmaxf(hi3[2], r.z);
-            }
-        bool ok = finite && span_ok && (64 * k + 64 <= xe);
-        for (int a = 0; a < 3; ++a) {
-            const float lb = fmaxf(frame.lo[a], (float)frame.bl[a]) + 1.0f / 64.0f;
-            const float hb = fminf(frame.hi[a], (float)frame.bh[a]) - 1.0f / 64.0f;
-            ok = ok && lo3[a] >= lb && hi3[a] < hb;
-        }
-        segf[tid] = ok ? 1 : 0;
+    // Unchecked-path bounds per axis: every tap of a sample q with
+    // lb <= q < hb lies inside the volume and the source buffer.
+    float lb[3], hb[3];
+    for (int a = 0; a < 3; ++a) {
+        lb[a] = fmaxf(frame.lo[a], (float)frame.bl[a]) + 1.0f / 64.0f;
+        hb[a] = fminf(frame.hi[a], (float)frame.bh[a]) - 1.0f / 64.0f;
     }
-    __syncthreads();
+    // per row segment (row y, 64 voxels 64k..64k+63): may it skip the bounds
+    // checks in x and y?  (z is decided per output slice below.)
+    const int64_t xe = J.out_o[0] + J.out_n[0] - O[0];  // valid x extent in this brick
+    const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
+    bool seg_ok = true;
+    if (tid < Gm::BY * 4) {
+        const int y = tid >> 2, k = tid & 3;
+        const float qx0 = (float)(64 * k) + dmn[0], qx1 = (float)(64 * k + 63) + dmx[0];
+        const float qy0 = (float)y + dmn[1], qy1 = (float)y + dmx[1];
+        // (rows at or beyond ye are never written, so they need no test)
+        seg_ok = (y >= ye) || (span_ok && (64 * k + 64 <= xe) && qx0 >= lb[0] && qx1 < hb[0] && qy0 >= lb[1] &&
+                               qy1 < hb[1]);
+        segf[tid] = seg_ok ? 1 : 0;
+    }
+    // every segment of the brick is unchecked in x and y
+    const bool xy_fast = __syncthreads_and(seg_ok) != 0;  // also publishes R and segf
+    // slice z (at brick position pz) is unchecked in z when zlo <= pz < zhi
+    // (folding DF into the bounds moves them by far less than the margin)
+    const float zlo = lb[2] - dmn[2], zhi = hb[2] - dmx[2];
 
     const T *src = static_cast<const T *>(J.src);
     T *dst = static_cast<T *>(J.dst);
@@ -743,7 +774,7 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     B.pz = J.src_pz;
     B.frame = frame;
     B.cw = cw;
-    B.rows = make_rows(B.base, B.py32, B.pz32);
+    B.rows = make_rows(B.base, B.py32, B.pz32, mn, span_ok);
     // x weights of the lane's voxel pair (2l, 2l+1) + 64k: the brick origin is
     // a multiple of G and G divides 64, so they do not depend on k
     B.wx[0] = W[(2 * tx) % G];
@@ -752,7 +783,6 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     // a voxel pair (even x) can be written as one 2-element store
     B.pair_ok = ((((uintptr_t)(dst + dbase0)) % (2 * sizeof(T))) == 0) && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
     B.xe = (int)xe;
-    const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
     const int64_t ze = J.out_o[2] + J.out_n[2] - zfirst;
 
     for (int z = 0; z < zs; ++z) {
@@ -771,12 +801,18 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
         }
         __syncthreads();
         if (z >= ze) continue;  // uniform: whole slice outside the region
-        // fast bricks skip the per-segment flags; otherwise each warp-row
-        // segment picks its path (uniform across the warp)
-        if (fast)
-            tps_rows<T, G, INTERP, true>(Q, B, tx, ty, (int)ye, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, segf);
+        // z of this slice: q_z lies in zoff + z + [min DF_z, max DF_z]
+        const float pz = (float)(zoff + z);
+        const bool z_fast = pz >= zlo && pz < zhi;
+        // a slice whose every segment is unchecked skips the per-segment
+        // flags; otherwise each warp-row segment picks its path (uniform
+        // across the warp)
+        if (xy_fast && z_fast)
+            tps_rows<T, G, INTERP, true>(Q, B, tx, ty, (int)ye, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, segf,
+                                         true);
         else
-            tps_rows<T, G, INTERP, false>(Q, B, tx, ty, (int)ye, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, segf);
+            tps_rows<T, G, INTERP, false>(Q, B, tx, ty, (int)ye, dst + dbase0 + (int64_t)z * J.dst_pz, J.dst_py, segf,
+                                          z_fast);
     }
     __syncthreads();  // smem reuse by the next brick
 }
@@ -791,7 +827,7 @@ template <typename T, int INTERP, bool FAST>
 __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float (&fo)[3], int lane, int ty, int ye,
                                             int ze, int xe, const T *base, int py32, int pz32, int64_t py, int64_t pz,
                                             const Frame &frame, const Clamp &cw, T *dbrick, int64_t dpy, int64_t dpz,
-                                            bool pair_ok)
+                                            bool pair_ok, const Rows<T> &rows)
 {
 #pragma unroll 1
     for (int z = 0; z < kABZ; ++z) {
@@ -815,7 +851,7 @@ __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float 
                 const float2 pz2 = f2(qz0, qz0 + m[2][0]);
                 uint32_t w;
                 if (FAST)
-                    pair_fast2<T, false>(p0, p1, pz2, make_rows(base, py32, pz32), w);
+                    pair_fast2<T, false>(p0, p1, pz2, rows, w);
                 else if (cw.span32)
                     pair_checked2<T, false, int>(p0, p1, pz2, base, py32, pz32, frame, cw.cl, cw.ch, xe - x, w);
                 else
@@ -895,18 +931,19 @@ __device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, 
     const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
     const int64_t ze = J.out_o[2] + J.out_n[2] - O[2];
     const Clamp cw = make_clamp(J, frame, lo, hi);
+    const Rows<T> rows = make_rows(base, py32, pz32, lo, fast);
     if (fast)
         affine_rows<T, INTERP, true>(m, fo, tx, ty, (int)ye, (int)ze, (int)xe, base, py32, pz32, J.src_py, J.src_pz,
-                                     frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok);
+                                     frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok, rows);
     else
         affine_rows<T, INTERP, false>(m, fo, tx, ty, (int)ye, (int)ze, (int)xe, base, py32, pz32, J.src_py, J.src_pz,
-                                      frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok);
+                                      frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok, rows);
 }
 
 // ---------------------------------------------------------------- kernels
 
 template <typename T, int G, int INTERP>
-__global__ void __launch_bounds__(kThreads, 3) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
+__global__ void __launch_bounds__(kThreads, TW_RES_MINB) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
                                                             int64_t total_bricks)
 {
     extern __shared__ float4 smem[];
