@@ -14,6 +14,10 @@ FP32 compensated node evaluation, fused B-spline + trilinear resample.
           per node) / its measured duration vs MEASURED_PEAKS.json hbm_gbs
   cpu_baseline  the FP64 oracle (a restatement of the reference's CPU path)
           on a bounded slab of the same job, extrapolated, all host threads
+  serving the serving mix (Poisson arrivals, mixed affine/rigid/TPS jobs of
+          uneven sizes) through the continuous-batching server: p50/p99 job
+          latency and aggregate GVoxel/s, capacity with every job submitted at
+          once, and the plain one-job-at-a-time path on the same jobs
 
 The volume (8 GiB) is far larger than L2 (126 MB), so no flush is needed
 between iterations.  `--impl reference` times the reference's CPU path (the
@@ -53,6 +57,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-jobs", type=int, default=32, help="jobs in the serving leg")
     ap.add_argument("--small", action="store_true", help="256x256x128 case, 64 landmarks")
     ap.add_argument("--shape", type=str, default="", help="X,Y,Z volume for profiling captures (default: full)")
     return ap.parse_args()
@@ -214,6 +220,88 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------- serving leg
+
+def serving_leg(ctx, device: int, n_jobs: int, seed: int = 1239, rate_hz: float = 20.0):
+    """The serving mix (Poisson arrivals at rate_hz, dims log-uniform 128^3 ..
+    1024x1024x256, u8/u16, 30% affine / 10% rigid / 60% TPS with 16-4096
+    landmarks) through the continuous-batching server from pinned host
+    buffers: p50/p99 job latency (submit to result in host memory) and
+    aggregate GVoxel/s; the same jobs submitted all at once (capacity); and the
+    plain one-job-at-a-time path (operator-level call per job, H2D and D2H
+    included) for comparison."""
+    import numpy as np
+    import torch
+
+    import terawarp_b200 as tw
+    from terawarp_b200 import api, synth
+
+    dev = f"cuda:{device}"
+    jobs = synth.serving_jobs(n_jobs, seed=seed, rate_hz=rate_hz)
+    tdt = {"u8": torch.uint8, "u16": torch.uint16}
+    esz = {"u8": 1, "u16": 2}
+    nbytes = [int(np.prod(j.shape_zyx)) * esz[j.dtype] for j in jobs]
+    # inputs: views of one pinned pool of random bytes (jobs only read them)
+    pool = torch.empty(max(nbytes), dtype=torch.uint8, pin_memory=True)
+    pool.copy_(torch.randint(0, 256, (max(nbytes),), dtype=torch.uint8, device=dev))
+    srcs = [pool[:b].view(tdt[j.dtype]).reshape(j.shape_zyx) for j, b in zip(jobs, nbytes)]
+    outs = [torch.empty(j.shape_zyx, dtype=tdt[j.dtype], pin_memory=True) for j in jobs]
+    vox = sum(int(np.prod(j.shape_zyx)) for j in jobs)
+
+    def submit(srv, j, src, dst):
+        if j.kind == "tps":
+            return srv.submit_tps(j.centres, j.values, j.g, src, dst)
+        return srv.submit_affine(j.M, src, dst)
+
+    def plain(j, src, dst):
+        if j.kind == "tps":
+            tw.imgwarp_smallmemory_image(ctx, j.values, j.centres, j.g, j.g, j.g, 1, 0, src, out=dst)
+        else:
+            d_src = src.to(dev, non_blocking=True)
+            d_dst = torch.empty_like(d_src)
+            tw.warp_affine_device(ctx, j.M, d_src, d_dst)
+            dst.copy_(d_dst)
+        torch.cuda.synchronize()
+
+    warm = list(range(min(4, n_jobs)))
+    with api.Server(ctx) as srv:
+        for i in warm:
+            srv.wait(submit(srv, jobs[i], srcs[i], outs[i]))
+        # Poisson arrivals
+        t0 = time.perf_counter()
+        ids = []
+        for j, src, dst in zip(jobs, srcs, outs):
+            delay = t0 + j.arrival_s - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(submit(srv, j, src, dst))
+        lats = [srv.wait(i) for i in ids]
+        t_poisson = time.perf_counter() - t0
+        # capacity: every job submitted at once
+        t0 = time.perf_counter()
+        ids = [submit(srv, j, src, dst) for j, src, dst in zip(jobs, srcs, outs)]
+        for i in ids:
+            srv.wait(i)
+        t_sat = time.perf_counter() - t0
+    for i in warm:
+        plain(jobs[i], srcs[i], outs[i])
+    t0 = time.perf_counter()
+    for j, src, dst in zip(jobs, srcs, outs):
+        plain(j, src, dst)
+    t_seq = time.perf_counter() - t0
+    lat_ms = sorted(1e3 * v for v in lats)
+    kinds = {k: sum(1 for j in jobs if j.kind == k) for k in ("affine", "rigid", "tps")}
+    return {
+        "jobs": n_jobs, "rate_hz": rate_hz, "mix": kinds, "voxels": vox,
+        "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+        "poisson_gvoxel_s": vox / t_poisson / 1e9, "poisson_wall_s": t_poisson,
+        "saturated_gvoxel_s": vox / t_sat / 1e9,
+        "sequential_gvoxel_s": vox / t_seq / 1e9,
+        "saturated_over_sequential": t_seq / t_sat,
+        "path": "tw_server_* from pinned host buffers vs one operator-level call per job",
+    }
+
+
 # ----------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -341,6 +429,8 @@ def run_ours(args):
         equal = bool(torch.equal(h_dst, dst.cpu()))
         line["e2e"]["matches_device_path"] = equal
         del h_src, h_dst
+    if rank == 0 and not args.no_serve and not args.small and not args.shape:
+        line["serving"] = serving_leg(ctx, local, args.serve_jobs)
     if rank == 0 and ws == 1 and not args.no_cpu and not args.small and not args.shape:
         from oracle import oracle as O
         slab_planes = 8
