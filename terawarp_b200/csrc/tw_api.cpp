@@ -123,9 +123,12 @@ bool is_pinned_ptr(const void *p)
     return a.type == cudaMemoryTypeHost;
 }
 
+// Device aux block of a TPS: d (16 doubles) then the status word.
+static constexpr size_t kTpsAuxBytes = sizeof(double) * 16 + 16;
+
 // Device-resident TPS field of one job: coefficients + node grid.
 tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *values, int n, double lambda,
-                   double scale, cudaStream_t st, tw_tps **out)
+                   double scale, cudaStream_t st, tw_tps **out, bool wait)
 {
     *out = nullptr;
     if (!centres || !values || n < 4) return fail(ctx, TW_ERR_ARG, "TPS needs n >= 4 landmark pairs");
@@ -152,12 +155,17 @@ tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *value
     tw_status s = dmalloc_on(ctx, (void **)&t->d_c, cbytes, st);
     if (s == TW_OK) s = dmalloc_on(ctx, (void **)&t->d_ctr32, fbytes, st);
     if (s == TW_OK) s = dmalloc_on(ctx, (void **)&t->d_coef32, fbytes, st);
-    if (s == TW_OK)
-        s = solve_tps_device(ctx, hc.data(), hv.data(), n, lambda, t->d_c, t->h_d, o, t->d_ctr32, t->d_coef32, st);
+    if (s == TW_OK) s = dmalloc_on(ctx, (void **)&t->d_d, kTpsAuxBytes, st);
+    if (s == TW_OK) {
+        t->d_status = reinterpret_cast<int *>(t->d_d + 16);
+        s = solve_tps_device(ctx, hc.data(), hv.data(), n, lambda, t->d_c, t->d_d, t->d_status,
+                             wait ? t->h_d : nullptr, o, t->d_ctr32, t->d_coef32, st);
+    }
     if (s != TW_OK) {
         dfree_on(ctx, t->d_c, cbytes, st);
         dfree_on(ctx, t->d_ctr32, fbytes, st);
         dfree_on(ctx, t->d_coef32, fbytes, st);
+        dfree_on(ctx, t->d_d, kTpsAuxBytes, st);
         return s;
     }
     for (int a = 0; a < 3; ++a) t->o32[a] = o[a];
@@ -174,6 +182,7 @@ void destroy_tps(tw_tps *t)
     dfree(ctx, t->d_c, sizeof(double) * 4 * (size_t)t->n);
     dfree(ctx, t->d_ctr32, sizeof(float4) * (size_t)t->n);
     dfree(ctx, t->d_coef32, sizeof(float4) * (size_t)t->n);
+    dfree(ctx, t->d_d, kTpsAuxBytes);
     delete[] t->h_ctr;
     delete t;
 }
@@ -185,16 +194,10 @@ tw_status eval_grid(tw_ctx *ctx, const tw_tps *t, const int64_t gsz[3], int g, c
     p.ctr = t->d_ctr32;
     p.coef = t->d_coef32;
     p.n = t->n;
-    const double *d = t->h_d;
-    // f_c(p) = d[0][c] + sum_r p_r d[r+1][c];  with p = o + p':
-    // DF_c = (d[0][c] + o.d[1:4][c] - o_c) + sum_r p'_r (d[r+1][c] - delta)
-    for (int c = 0; c < 3; ++c) {
-        double a0 = d[0 * 4 + c + 1];
-        for (int r = 0; r < 3; ++r) a0 += t->o32[r] * d[(r + 1) * 4 + c + 1];
-        a0 -= t->o32[c];
-        p.a0[c] = (float)a0;
-        for (int r = 0; r < 3; ++r) p.alin[r][c] = (float)(d[(r + 1) * 4 + c + 1] - (r == c ? 1.0 : 0.0));
-    }
+    // the affine part stays on the device (the kernel folds it with o), so an
+    // evaluation can follow an unwaited solve on the same stream
+    p.aff = t->d_d;
+    for (int a = 0; a < 3; ++a) p.o[a] = t->o32[a];
     for (int a = 0; a < 3; ++a) {
         p.gsz[a] = gsz[a];
         p.node_o[a] = (int64_t)(-g + off[a] - (int64_t)t->o32[a]);

@@ -109,13 +109,26 @@ __global__ void __launch_bounds__(kEvalThreads) k_tps_eval(EvalParams p)
         }
     }
 
+    // affine part: f_c(q) = d[0][c] + sum_r q_r d[r+1][c]; with q = o + p:
+    // DF_c = (d[0][c] + o.d[1:4][c] - o_c) + sum_r p_r (d[r+1][c] - delta),
+    // folded in FP64 without contraction, then rounded once to float
+    float a0[3], alin[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double s = __ldg(&p.aff[c + 1]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) s = __dadd_rn(s, __dmul_rn(p.o[r], __ldg(&p.aff[(r + 1) * 4 + c + 1])));
+        a0[c] = (float)__dsub_rn(s, p.o[c]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) alin[r][c] = (float)__dsub_rn(__ldg(&p.aff[(r + 1) * 4 + c + 1]), r == c ? 1.0 : 0.0);
+    }
 #pragma unroll
     for (int j = 0; j < kNPT; ++j) {
         const int64_t L = base + (int64_t)j * kEvalThreads;
         if (L >= nnodes) continue;
-        float dfx = p.a0[0] + p.alin[0][0] * px[j] + p.alin[1][0] * py[j] + p.alin[2][0] * pz[j];
-        float dfy = p.a0[1] + p.alin[0][1] * px[j] + p.alin[1][1] * py[j] + p.alin[2][1] * pz[j];
-        float dfz = p.a0[2] + p.alin[0][2] * px[j] + p.alin[1][2] * py[j] + p.alin[2][2] * pz[j];
+        float dfx = a0[0] + alin[0][0] * px[j] + alin[1][0] * py[j] + alin[2][0] * pz[j];
+        float dfy = a0[1] + alin[0][1] * px[j] + alin[1][1] * py[j] + alin[2][1] * pz[j];
+        float dfz = a0[2] + alin[0][2] * px[j] + alin[1][2] * py[j] + alin[2][2] * pz[j];
         // the running compensation holds minus the lost low-order part
         dfx += sx[j] - cx[j];
         dfy += sy[j] - cy[j];

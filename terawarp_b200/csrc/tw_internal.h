@@ -73,8 +73,8 @@ struct EvalParams {
     const float4 *ctr;     // n centres, relative to the job origin `o`
     const float4 *coef;    // n coefficients (-c_x, -c_y, -c_z, 0)
     int n;
-    float a0[3];           // affine part at the origin minus the origin
-    float alin[3][3];      // alin[r][c] = d[r+1][c+1] - delta(r,c)
+    const double *aff;     // device 4 x 4 FP64 affine part d of the TPS (row-major)
+    double o[3];           // the origin: a0 / alin are folded from aff and o on the device
     int64_t gsz[3];
     int g;
     int64_t node_o[3];     // position of node (0,0,0) relative to the origin
@@ -85,12 +85,18 @@ cudaError_t launch_tps_eval(const EvalParams &p, cudaStream_t st, int sm_count);
 // ------------------------------------------------------------------- solve
 
 struct SolveWork;   // device workspace of one solve
-// Solves on `st` and waits for it once, at the end.  When ctr32_out and
+// Solves on `st`: c into d_c_out (n x 4), d into d_d_out (4 x 4) and the
+// status bits into d_status_out, all device memory that outlives the call.
+// With h_d_out it waits for `st` once, at the end, copies d to the host and
+// turns the status into the return value; without it nothing waits and the
+// caller reads the status later (solve_status).  When ctr32_out and
 // coef32_out are given it also writes the FP32 evaluation arrays: centres
 // relative to `o` and the negated non-affine coefficients (-c_x, -c_y, -c_z).
 tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
-                           double *d_c_out /*n x 4 device*/, double *h_d_out /*4x4 host*/,
+                           double *d_c_out, double *d_d_out, int *d_status_out, double *h_d_out,
                            const double o[3], float4 *ctr32_out, float4 *coef32_out, cudaStream_t st);
+// The status word of a solve as a tw_status (waits for `st`).
+tw_status solve_status(tw_ctx *ctx, const int *d_status, cudaStream_t st);
 tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_sub, int n, double M[16],
                             cudaStream_t st);
 // The affine fit kernel alone on caller-provided device buffers (d_status
@@ -143,7 +149,9 @@ struct tw_tps {
     tw_ctx *ctx = nullptr;
     int n = 0;
     double *d_c = nullptr;     // device n x 4 (FP64)
-    double h_d[16] = {0};      // host 4 x 4 (FP64)
+    double h_d[16] = {0};      // host 4 x 4 (FP64), valid once the solve was waited for
+    double *d_d = nullptr;     // device 4 x 4 (FP64)
+    int *d_status = nullptr;   // device solve status bits
     float4 *d_ctr32 = nullptr; // centres, FP32, relative to origin o32
     float4 *d_coef32 = nullptr;
     double o32[3] = {0, 0, 0};

@@ -68,6 +68,9 @@ struct tw_server {
     std::vector<JobRec *> active;
     std::vector<cudaStream_t> streams;
     cudaStream_t batch = nullptr;
+    // all solves run on this one stream, one after another: each is a
+    // cooperative kernel that wants every SM, and they are short
+    cudaStream_t solve_st = nullptr;
     uint64_t next_id = 1;
     bool stop = false;
     std::thread worker;
@@ -126,9 +129,13 @@ tw_status prepare(tw_server *s, JobRec *j)
     TW_CUDA_TRY(cudaEventCreateWithFlags(&j->ev_ready, cudaEventDisableTiming));
     TW_CUDA_TRY(cudaEventCreateWithFlags(&j->ev_done, cudaEventDisableTiming));
     if (sp.kind == 1) {
-        // solve first: its host synchronisation then waits for the solve only
-        TW_TRY(make_tps(ctx, j->ctr.data(), j->val.data(), sp.n, sp.lambda > 0 ? sp.lambda : 0.2, 1.0, j->st,
-                        &j->tps));
+        // the solve (on the solve stream), the node grid and the upload (on
+        // the job's stream) are queued without a host wait; the solve's status
+        // is read at completion
+        TW_TRY(make_tps(ctx, j->ctr.data(), j->val.data(), sp.n, sp.lambda > 0 ? sp.lambda : 0.2, 1.0, s->solve_st,
+                        &j->tps, /*wait=*/false));
+        TW_CUDA_TRY(cudaEventRecord(j->ev_ready, s->solve_st));
+        TW_CUDA_TRY(cudaStreamWaitEvent(j->st, j->ev_ready, 0));
         const int64_t gsz[3] = {grid_size(sp.dst_sz[0], sp.g), grid_size(sp.dst_sz[1], sp.g),
                                 grid_size(sp.dst_sz[2], sp.g)};
         j->nodes_b = sizeof(float4) * (size_t)(gsz[0] * gsz[1] * gsz[2]);
@@ -235,8 +242,13 @@ void worker_main(tw_server *s)
             tw_status st = TW_OK;
             if (j->state == kComputing) {
                 cudaError_t e = cudaEventQuery(j->ev_done);
-                if (e == cudaSuccess) done = true;
-                else if (e != cudaErrorNotReady) { done = true; st = TW_ERR_CUDA; }
+                if (e == cudaSuccess) {
+                    done = true;
+                    if (j->tps) st = solve_status(s->ctx, j->tps->d_status, j->st);  // stream is idle: no wait
+                } else if (e != cudaErrorNotReady) {
+                    done = true;
+                    st = TW_ERR_CUDA;
+                }
             } else if (j->state == kPrepared && j->status != TW_ERR_NOT_READY) {
                 done = true;
                 st = j->status;
@@ -267,7 +279,9 @@ tw_status tw_server_create(tw_ctx *ctx, size_t hbm_budget_bytes, int max_infligh
     TW_TRY(tw_ctx_create(ctx->device, 0, &s->ctx));
     s->budget = hbm_budget_bytes ? hbm_budget_bytes : s->ctx->budget / 2;
     s->max_inflight = max_inflight > 0 ? max_inflight : 16;
-    if (cudaStreamCreateWithFlags(&s->batch, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&s->batch, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->solve_st, cudaStreamNonBlocking) != cudaSuccess) {
+        if (s->batch) cudaStreamDestroy(s->batch);
         tw_ctx_destroy(s->ctx);
         return TW_ERR_CUDA;
     }
@@ -348,11 +362,13 @@ tw_status tw_server_destroy(tw_server *s)
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->batch);
+    cudaStreamSynchronize(s->solve_st);
     for (cudaStream_t st : s->streams) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
     }
     cudaStreamDestroy(s->batch);
+    cudaStreamDestroy(s->solve_st);
     tw_ctx_destroy(s->ctx);
     delete s;
     return TW_OK;

@@ -717,12 +717,13 @@ struct StreamBuf {
 }  // namespace
 
 tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
-                           double *d_c_out, double *h_d_out, const double o[3], float4 *ctr32_out,
-                           float4 *coef32_out, cudaStream_t st)
+                           double *d_c_out, double *d_d_out, int *d_status_out, double *h_d_out, const double o[3],
+                           float4 *ctr32_out, float4 *coef32_out, cudaStream_t st)
 {
     const int m = n - 4;
     // workspace: ctr 3n, Y 4n, Xw 4n, V 4n, P 4n, W 4n, Z 4n, KC 4n, tau 4, R 16, d 16, status
-    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + 16 + 2 + 2;
+    // ctr 3n, Y/Xw/V/P/W/Z/KC 4n each, tau 4, R 16, grid barrier 2
+    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + 2;
     // stream-ordered workspace on `st`, returned to the pool on `st` when this
     // function exits (after the final wait, or with the error)
     StreamBuf ws{ctx, st}, abuf{ctx, st};
@@ -739,9 +740,9 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
     double *d_KC = d_Z + 4 * (size_t)n;
     double *d_tau = d_KC + 4 * (size_t)n;
     double *d_R = d_tau + 4;
-    double *d_d = d_R + 16;
-    int *d_status = reinterpret_cast<int *>(d_d + 16);
-    GridBar *d_bar = reinterpret_cast<GridBar *>(d_d + 18);  // 16 bytes, 8-byte aligned
+    double *d_d = d_d_out;
+    int *d_status = d_status_out;
+    GridBar *d_bar = reinterpret_cast<GridBar *>(d_R + 16);  // 16 bytes, 8-byte aligned
     if (m > 0) {
         abuf.bytes = (size_t)(m + 4) * m * sizeof(double);
         TW_TRY(dmalloc_on(ctx, &abuf.p, abuf.bytes, st));
@@ -793,9 +794,15 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
     }
     TW_CUDA_TRY(cudaGetLastError());
     count_launch(ctx, nl);
+    if (!h_d_out) return TW_OK;  // the caller reads the status later
+    TW_CUDA_TRY(cudaMemcpyAsync(h_d_out, d_d, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
+    return solve_status(ctx, d_status, st);
+}
+
+tw_status solve_status(tw_ctx *ctx, const int *d_status, cudaStream_t st)
+{
     int status = 0;
     TW_CUDA_TRY(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    TW_CUDA_TRY(cudaMemcpyAsync(h_d_out, d_d, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
     TW_CUDA_TRY(cudaStreamSynchronize(st));
     if (status & kStSingularX)
         return fail(ctx, TW_ERR_SINGULAR, "TPS centres are degenerate: [1 s] is rank deficient (coplanar or < 4 distinct points)");
