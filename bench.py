@@ -406,6 +406,7 @@ def run_ours(args):
         "clocks": clocks,
         "stages_ms": {"solve_fp64": statistics.mean(solve_ms), "node_eval_fp32": eval_avg, "resample": warp_avg},
         "resample_ms_per_step": [round(v, 3) for v in warp_ms],
+        "solve_ms_per_step": [round(v, 3) for v in solve_ms],
         "tps_eval": {"pairs": pairs, "flop_per_pair": 15, "tflops": pairs * 15 / (eval_avg / 1e3) / 1e12,
                      "fp32_peak_tflops_at_clock": fp32_peak_tflops,
                      "frac": pairs * 15 / (eval_avg / 1e3) / 1e12 / fp32_peak_tflops},

@@ -37,7 +37,7 @@ namespace {
 
 constexpr int kThreads = 256;
 #ifndef TW_RES_MINB
-#define TW_RES_MINB 3  // resident CTAs per SM the TPS kernel is compiled for (register budget)
+#define TW_RES_MINB 4  // resident CTAs per SM the TPS kernel is compiled for (64 registers)
 #endif
 constexpr int kTX = 32;
 constexpr int kTY = 8;
@@ -458,11 +458,14 @@ __device__ __forceinline__ void pair_fast2(float2 p0, float2 p1, float2 pz2, con
     const float2 f0 = sub2(p0, sub2(m0, MM)), f1 = sub2(p1, sub2(m1, MM)), fz = sub2(pz2, sub2(mz, MM));
     const uint32_t off0 = tap_offset(R, m0.x, m0.y, mz.x);
     const uint32_t off1 = tap_offset(R, m1.x, m1.y, mz.y);
-    // magic floats of the 8 taps of both voxels
+    // magic floats of the 8 taps of both voxels: one wide address per voxel,
+    // the other rows at the brick's constant row / plane offsets
     float2 lo[4], hi[4];
+    const T *a0 = wide_addr(R.rb[0], off0), *a1 = wide_addr(R.rb[0], off1);
+    const int rofs[4] = {0, R.py, R.pz, R.py + R.pz};
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const T *q0 = wide_addr(R.rb[r], off0), *q1 = wide_addr(R.rb[r], off1);
+        const T *q0 = a0 + rofs[r], *q1 = a1 + rofs[r];
         lo[r] = f2(mag(q0), mag(q1));
         hi[r] = f2(mag(q0 + 1), mag(q1 + 1));
     }
