@@ -405,17 +405,14 @@ struct Rows {
     uint32_t k;  // magic-number bias and the hull corner folded out of the offsets
 };
 
-// lo: the hull's low corner relative to `base` (used only when `valid`, i.e.
-// when the brick has unchecked samples and all its offsets fit int32).
+// corner: the low corner (relative to `base`) of the box every tap of the
+// brick lies in -- the clamp window of its checked samples, which also holds
+// every unchecked tap -- so tap offsets from it are non-negative; used only
+// when `valid` (offsets within the box fit 32 bits).
 template <typename T>
-__device__ __forceinline__ Rows<T> make_rows(const T *base, int py, int pz, const float (&lo)[3], bool valid)
+__device__ __forceinline__ Rows<T> make_rows(const T *base, int py, int pz, const int (&corner)[3], bool valid)
 {
-    // one voxel of slack below the hull: a sample computed in FP32 may fall a
-    // rounding error below the exact bound
-    int il[3] = {0, 0, 0};
-    if (valid)
-        for (int a = 0; a < 3; ++a) il[a] = (int)floorf(lo[a]) - 1;
-    const int omin = il[2] * pz + il[1] * py + il[0];
+    const int omin = valid ? corner[2] * pz + corner[1] * py + corner[0] : 0;
     const T *b = base + omin;
     Rows<T> r;
     r.rb[0] = b;
@@ -428,7 +425,7 @@ __device__ __forceinline__ Rows<T> make_rows(const T *base, int py, int pz, cons
     return r;
 }
 
-// Element offset of floor(q) from the rows' hull corner, from the
+// Element offset of floor(q) from the rows' corner, from the
 // magic-floor bit patterns (2^32 wrap arithmetic; exact because the result
 // lies in [0, 2^31)).
 template <typename T>
@@ -449,15 +446,12 @@ __device__ __forceinline__ const T *wide_addr(const T *base, uint32_t o)
 
 // Unchecked sample of a voxel pair at positions (p0, p1, pz2): every tap is
 // known to be inside the volume and the buffer (hull test), offsets fit int32.
-template <typename T, bool ROUND>
-__device__ __forceinline__ void pair_fast2(float2 p0, float2 p1, float2 pz2, const Rows<T> &R, uint32_t &packed)
+// Trilinear value of a voxel pair from the offsets of its (0,0,0) taps and
+// its fractions (fx, fy, fz), as a pair (voxel 0, voxel 1).
+template <typename T>
+__device__ __forceinline__ float2 lerp_pair(const Rows<T> &R, uint32_t off0, uint32_t off1, float2 fx, float2 fy,
+                                            float2 fz)
 {
-    const float2 MM = f2(kMagic, kMagic);
-    // floor via add.rm of 1.5*2^23, fractions
-    const float2 m0 = __fadd2_rd(p0, MM), m1 = __fadd2_rd(p1, MM), mz = __fadd2_rd(pz2, MM);
-    const float2 f0 = sub2(p0, sub2(m0, MM)), f1 = sub2(p1, sub2(m1, MM)), fz = sub2(pz2, sub2(mz, MM));
-    const uint32_t off0 = tap_offset(R, m0.x, m0.y, mz.x);
-    const uint32_t off1 = tap_offset(R, m1.x, m1.y, mz.y);
     // magic floats of the 8 taps of both voxels: one wide address per voxel,
     // the other rows at the brick's constant row / plane offsets
     float2 lo[4], hi[4];
@@ -469,21 +463,70 @@ __device__ __forceinline__ void pair_fast2(float2 p0, float2 p1, float2 pz2, con
         lo[r] = f2(mag(q0), mag(q1));
         hi[r] = f2(mag(q0 + 1), mag(q1 + 1));
     }
-    const float2 fx = f2(f0.x, f1.x), fy = f2(f0.y, f1.y);
     float2 ax[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)  // (2^23 + b) - (2^23 + a) = b - a exactly
         ax[r] = fma2(fx, sub2(hi[r], lo[r]), sub2(lo[r], f2(8388608.f, 8388608.f)));
     const float2 b0 = fma2(fy, sub2(ax[1], ax[0]), ax[0]);
     const float2 b1 = fma2(fy, sub2(ax[3], ax[2]), ax[2]);
-    float2 v = fma2(fz, sub2(b1, b0), b0);
-    // v is a convex combination of voxel values; rounding can leave -0.0x
+    return fma2(fz, sub2(b1, b0), b0);
+}
+
+// Output words of a voxel pair: TPS rounds (+0.5), affine truncates; v is a
+// convex combination of voxel values (rounding can leave -0.0x), so
+// 2^23 + floor(v) has the output in its low bits.
+template <typename T, bool ROUND>
+__device__ __forceinline__ float2 out_pair(float2 v)
+{
     if (ROUND) v = add2(v, f2(0.5f, 0.5f));
     else v = f2(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f));
-    // 2^23 + floor(v): floor(v) lies in [0, max of T] (v never exceeds the
-    // largest tap by more than an ulp), so its low bits are the output
-    const float2 t = __fadd2_rd(v, f2(8388608.f, 8388608.f));
+    return __fadd2_rd(v, f2(8388608.f, 8388608.f));
+}
+
+template <typename T, bool ROUND>
+__device__ __forceinline__ void pair_fast2(float2 p0, float2 p1, float2 pz2, const Rows<T> &R, uint32_t &packed)
+{
+    const float2 MM = f2(kMagic, kMagic);
+    // floor via add.rm of 1.5*2^23, fractions
+    const float2 m0 = __fadd2_rd(p0, MM), m1 = __fadd2_rd(p1, MM), mz = __fadd2_rd(pz2, MM);
+    const float2 f0 = sub2(p0, sub2(m0, MM)), f1 = sub2(p1, sub2(m1, MM)), fz = sub2(pz2, sub2(mz, MM));
+    const uint32_t off0 = tap_offset(R, m0.x, m0.y, mz.x);
+    const uint32_t off1 = tap_offset(R, m1.x, m1.y, mz.y);
+    const float2 t = out_pair<T, ROUND>(lerp_pair(R, off0, off1, f2(f0.x, f1.x), f2(f0.y, f1.y), fz));
     packed = pack_pair<T>(__float_as_uint(t.x), __float_as_uint(t.y));
+}
+
+// Checked sample of a voxel pair with 32-bit offsets: the reference's range
+// test per voxel (0 <= q <= sz-1 in every axis, else 0), and floor(q) clamped
+// to [cl, ch-1] of the clamp window so that both taps of every axis are
+// inside it.  For a valid sample the clamp changes nothing except at q =
+// sz-1 exactly, where floor sz-2 with fraction 1 gives the same value as the
+// reference's floor sz-1 with fraction 0 (lo + 1 (hi - lo) = hi exactly).
+// Needs ch > cl in every axis.
+template <typename T, bool ROUND>
+__device__ __forceinline__ void pair_clamped2(float2 p0, float2 p1, float2 pz2, const Rows<T> &R, const Frame &f,
+                                              const int (&cl)[3], const int (&ch)[3], int nvalid, uint32_t &packed)
+{
+    const float2 MM = f2(kMagic, kMagic);
+    const bool ok0 = nvalid >= 1 && p0.x >= f.lo[0] && p0.x <= f.hi[0] && p0.y >= f.lo[1] && p0.y <= f.hi[1] &&
+                     pz2.x >= f.lo[2] && pz2.x <= f.hi[2];
+    const bool ok1 = nvalid >= 2 && p1.x >= f.lo[0] && p1.x <= f.hi[0] && p1.y >= f.lo[1] && p1.y <= f.hi[1] &&
+                     pz2.y >= f.lo[2] && pz2.y <= f.hi[2];
+    const float lx = (float)cl[0], ly = (float)cl[1], lz = (float)cl[2];
+    const float hx = (float)(ch[0] - 1), hy = (float)(ch[1] - 1), hz = (float)(ch[2] - 1);
+    // floors (NaN or huge positions clamp into the window; such voxels are
+    // rejected by the range test above)
+    float2 l0 = sub2(__fadd2_rd(p0, MM), MM), l1 = sub2(__fadd2_rd(p1, MM), MM), lz2 = sub2(__fadd2_rd(pz2, MM), MM);
+    l0 = f2(fminf(fmaxf(l0.x, lx), hx), fminf(fmaxf(l0.y, ly), hy));
+    l1 = f2(fminf(fmaxf(l1.x, lx), hx), fminf(fmaxf(l1.y, ly), hy));
+    lz2 = f2(fminf(fmaxf(lz2.x, lz), hz), fminf(fmaxf(lz2.y, lz), hz));
+    const float2 f0 = sub2(p0, l0), f1 = sub2(p1, l1), fz = sub2(pz2, lz2);
+    const float2 m0 = add2(l0, MM), m1 = add2(l1, MM), mz = add2(lz2, MM);  // exact: integers
+    const uint32_t off0 = tap_offset(R, m0.x, m0.y, mz.x);
+    const uint32_t off1 = tap_offset(R, m1.x, m1.y, mz.y);
+    const float2 t = out_pair<T, ROUND>(lerp_pair(R, off0, off1, f2(f0.x, f1.x), f2(f0.y, f1.y), fz));
+    // a rejected voxel writes 0: the bits of 2^23 have zero low bits
+    packed = pack_pair<T>(ok0 ? __float_as_uint(t.x) : 0x4B000000u, ok1 ? __float_as_uint(t.y) : 0x4B000000u);
 }
 
 // Checked sample of a voxel pair near the volume or buffer border: the same
@@ -548,7 +591,8 @@ __device__ __forceinline__ void pair_checked2(float2 p0, float2 p1, float2 pz2, 
 // brick's sample hull (+1), and whether offsets inside it fit int32.
 struct Clamp {
     int cl[3], ch[3];
-    bool span32;
+    bool span32;   // offsets within the window fit 32 bits (the rows' corner is cl)
+    bool clamped;  // span32 and at least two taps wide in every axis: pair_clamped2 applies
 };
 
 __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const float (&mn)[3], const float (&mx)[3])
@@ -566,6 +610,7 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
         span += fmax(fabs((double)l), fabs((double)h)) * pitch[a];
     }
     c.span32 = span < 1.0e9 && J.src_pz < 0x3fffffff;
+    c.clamped = c.span32 && c.ch[0] > c.cl[0] && c.ch[1] > c.cl[1] && c.ch[2] > c.cl[2];
     return c;
 }
 
@@ -601,7 +646,9 @@ __device__ __forceinline__ void tps_pair(const float4 *Q, const BrickCtx<T> &B, 
             store_packed<T>(drow + x, w, B.pair_ok, 2);
         } else {
             const int nv = B.xe - x;
-            if (B.cw.span32)
+            if (B.cw.clamped)
+                pair_clamped2<T, true>(p0, p1, pz2, B.rows, B.frame, B.cw.cl, B.cw.ch, nv, w);
+            else if (B.cw.span32)
                 pair_checked2<T, true, int>(p0, p1, pz2, B.base, B.py32, B.pz32, B.frame, B.cw.cl, B.cw.ch, nv, w);
             else
                 pair_checked2<T, true, int64_t>(p0, p1, pz2, B.base, B.py, B.pz, B.frame, B.cw.cl, B.cw.ch, nv, w);
@@ -754,7 +801,7 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
         const float qx0 = (float)(64 * k) + dmn[0], qx1 = (float)(64 * k + 63) + dmx[0];
         const float qy0 = (float)y + dmn[1], qy1 = (float)y + dmx[1];
         // (rows at or beyond ye are never written, so they need no test)
-        seg_ok = (y >= ye) || (span_ok && (64 * k + 64 <= xe) && qx0 >= lb[0] && qx1 < hb[0] && qy0 >= lb[1] &&
+        seg_ok = (y >= ye) || (span_ok && cw.span32 && (64 * k + 64 <= xe) && qx0 >= lb[0] && qx1 < hb[0] && qy0 >= lb[1] &&
                                qy1 < hb[1]);
         segf[tid] = seg_ok ? 1 : 0;
     }
@@ -777,7 +824,7 @@ __device__ void tps_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, flo
     B.pz = J.src_pz;
     B.frame = frame;
     B.cw = cw;
-    B.rows = make_rows(B.base, B.py32, B.pz32, mn, span_ok);
+    B.rows = make_rows(B.base, B.py32, B.pz32, cw.cl, cw.span32);
     // x weights of the lane's voxel pair (2l, 2l+1) + 64k: the brick origin is
     // a multiple of G and G divides 64, so they do not depend on k
     B.wx[0] = W[(2 * tx) % G];
@@ -855,6 +902,8 @@ __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float 
                 uint32_t w;
                 if (FAST)
                     pair_fast2<T, false>(p0, p1, pz2, rows, w);
+                else if (cw.clamped)
+                    pair_clamped2<T, false>(p0, p1, pz2, rows, frame, cw.cl, cw.ch, xe - x, w);
                 else if (cw.span32)
                     pair_checked2<T, false, int>(p0, p1, pz2, base, py32, pz32, frame, cw.cl, cw.ch, xe - x, w);
                 else
@@ -934,8 +983,8 @@ __device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, 
     const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
     const int64_t ze = J.out_o[2] + J.out_n[2] - O[2];
     const Clamp cw = make_clamp(J, frame, lo, hi);
-    const Rows<T> rows = make_rows(base, py32, pz32, lo, fast);
-    if (fast)
+    const Rows<T> rows = make_rows(base, py32, pz32, cw.cl, cw.span32);
+    if (fast && cw.span32)  // the unchecked path addresses taps from the rows' corner
         affine_rows<T, INTERP, true>(m, fo, tx, ty, (int)ye, (int)ze, (int)xe, base, py32, pz32, J.src_py, J.src_pz,
                                      frame, cw, dst + dbase0, J.dst_py, J.dst_pz, pair_ok, rows);
     else
