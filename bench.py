@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-affine", action="store_true", help="skip the affine leg")
+    ap.add_argument("--no-tiled", action="store_true", help="skip the tiled (out-of-core) leg")
     ap.add_argument("--serve-jobs", type=int, default=32, help="jobs in the serving leg")
     ap.add_argument("--small", action="store_true", help="256x256x128 case, 64 landmarks")
     ap.add_argument("--shape", type=str, default="", help="X,Y,Z volume for profiling captures (default: full)")
@@ -219,6 +221,72 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": "GVoxel/s", "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": "GVoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------- other legs
+
+def affine_leg(ctx, device: int, steps: int = 5):
+    """The affine configuration: a 1024 x 1024 x 512 uint16 blob+fibre volume
+    warped by the 12-parameter affine fitted from 32 landmark pairs, device
+    resident; CUDA-event time per warp and its HBM roofline (2 x 2 B per
+    output voxel)."""
+    import torch
+
+    import terawarp_b200 as tw
+    from terawarp_b200 import synth
+
+    case = synth.affine_case(device=f"cuda:{device}")
+    src = case.vol
+    dst = torch.empty_like(src)
+    M = tw.fit_affine(ctx, case.marker_tar, case.marker_sub)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        tw.warp_affine_device(ctx, M, src, dst, 0, stream=stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(steps):
+        tw.warp_affine_device(ctx, M, src, dst, 0, stream=stream)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    vox = src.numel()
+    peak, _ = measured_peaks()
+    gbs = vox * 4 / (ms / 1e3) / 1e9
+    del src, dst
+    return {"workload": "affine_1024x1024x512_u16_n32", "ms_per_warp": ms, "gvoxel_s": vox / (ms / 1e3) / 1e9,
+            "achieved_gbs": gbs, "frac_of_hbm": gbs / peak, "kernel": "k_resample_affine<uint16,trilinear>"}
+
+
+def tiled_leg(ctx, device: int, shape_zyx=(512, 2048, 2048), tile=(512, 512, 512), depth: int = 2):
+    """The out-of-core TPS path: a 2048 x 2048 x 512 uint16 volume in pinned
+    host memory (2000 landmarks, g = 16) warped tile by tile (512^3 output
+    tiles, source boxes = the tiles' exact sample footprints, staging depth
+    2): solve, node grid, reads, H2D, kernels, D2H and writes all inside the
+    wall-clock time."""
+    import torch
+
+    from terawarp_b200 import api, synth
+
+    Z, Y, X = shape_zyx
+    vol = synth.blob_volume(shape_zyx, "u16", SEED + 11, n_blobs=5000, n_fibres=1000, device=f"cuda:{device}")
+    h_src = torch.empty(shape_zyx, dtype=torch.uint16, pin_memory=True)
+    h_src.copy_(vol)
+    del vol
+    h_out = torch.empty(shape_zyx, dtype=torch.uint16, pin_memory=True)
+    sub, tar = synth.lattice_landmarks((X, Y, Z), N_LANDMARKS, SEED + 12)
+    # reference argument order: (ql_marker_tar = values, ql_marker_sub = centres)
+    api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, G, h_src, out=h_out, tile=tile, depth=depth)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, G, h_src, out=h_out, tile=tile, depth=depth)
+    torch.cuda.synchronize()
+    s = time.perf_counter() - t0
+    vox = X * Y * Z
+    del h_src, h_out
+    return {"workload": f"tiled_tps_{X}x{Y}x{Z}_u16_n{N_LANDMARKS}_g{G}", "tile_xyz": list(tile[::-1]),
+            "staging_depth": depth, "seconds": s, "gvoxel_s": vox / s / 1e9,
+            "path": "tw_imgwarp_smallmemory_tiled, pinned host volumes (built-in box reader/writer)"}
 
 
 # ------------------------------------------------------------- serving leg
@@ -433,6 +501,10 @@ def run_ours(args):
         equal = bool(torch.equal(h_dst, dst.cpu()))
         line["e2e"]["matches_device_path"] = equal
         del h_src, h_dst
+    if rank == 0 and not args.no_affine and not args.small and not args.shape:
+        line["affine"] = affine_leg(ctx, local)
+    if rank == 0 and not args.no_tiled and not args.small and not args.shape:
+        line["tiled"] = tiled_leg(ctx, local)
     if rank == 0 and not args.no_serve and not args.small and not args.shape:
         line["serving"] = serving_leg(ctx, local, args.serve_jobs)
     if rank == 0 and ws == 1 and not args.no_cpu and not args.small and not args.shape:
