@@ -258,15 +258,15 @@ def affine_leg(ctx, device: int, steps: int = 5):
             "achieved_gbs": gbs, "frac_of_hbm": gbs / peak, "kernel": "k_resample_affine<uint16,trilinear>"}
 
 
-def tiled_leg(ctx, device: int, shape_zyx=(512, 2048, 2048), tile=(512, 512, 512), depth: int = 2):
+def tiled_leg(ctx, device: int, shape_zyx=(512, 2048, 2048)):
     """The out-of-core TPS path: a 2048 x 2048 x 512 uint16 volume in pinned
-    host memory (2000 landmarks, g = 16) warped tile by tile (512^3 output
-    tiles, source boxes = the tiles' exact sample footprints, staging depth
-    2): solve, node grid, reads, H2D, kernels, D2H and writes all inside the
-    wall-clock time."""
+    host memory (2000 landmarks, g = 16) warped tile by tile (source boxes =
+    the tiles' exact sample footprints) with the tile shape and staging depth
+    the autotuner picks on the volume's corner block: solve, node grid, reads,
+    H2D, kernels, D2H and writes all inside the wall-clock time."""
     import torch
 
-    from terawarp_b200 import api, synth
+    from terawarp_b200 import api, autotune, synth
 
     Z, Y, X = shape_zyx
     vol = synth.blob_volume(shape_zyx, "u16", SEED + 11, n_blobs=5000, n_fibres=1000, device=f"cuda:{device}")
@@ -276,6 +276,7 @@ def tiled_leg(ctx, device: int, shape_zyx=(512, 2048, 2048), tile=(512, 512, 512
     h_out = torch.empty(shape_zyx, dtype=torch.uint16, pin_memory=True)
     sub, tar = synth.lattice_landmarks((X, Y, Z), N_LANDMARKS, SEED + 12)
     # reference argument order: (ql_marker_tar = values, ql_marker_sub = centres)
+    tile, depth, table = autotune.tune_tiled_tps(ctx, sub, tar, 1.0, G, h_src)
     api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, G, h_src, out=h_out, tile=tile, depth=depth)  # warm
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -284,8 +285,9 @@ def tiled_leg(ctx, device: int, shape_zyx=(512, 2048, 2048), tile=(512, 512, 512
     s = time.perf_counter() - t0
     vox = X * Y * Z
     del h_src, h_out
-    return {"workload": f"tiled_tps_{X}x{Y}x{Z}_u16_n{N_LANDMARKS}_g{G}", "tile_xyz": list(tile[::-1]),
+    return {"workload": f"tiled_tps_{X}x{Y}x{Z}_u16_n{N_LANDMARKS}_g{G}", "tile_xyz": list(tile),
             "staging_depth": depth, "seconds": s, "gvoxel_s": vox / s / 1e9,
+            "autotune": [{"tile_xyz": list(t), "depth": d, "sample_s": round(x, 4)} for t, d, x in table],
             "path": "tw_imgwarp_smallmemory_tiled, pinned host volumes (built-in box reader/writer)"}
 
 
