@@ -309,13 +309,17 @@ __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, d
     const int r0 = kb * kNB;
     const int nb = min(kNB, m - r0);
     __syncthreads();
+#pragma unroll 4
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
         a[r][c] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
     }
     __syncthreads();
     const int t = threadIdx.x;
-    const int tr = (t >> 4) * 4, tc = (t & 15) * 4;
+    // thread t updates rows tr + 16u and columns tc + 16v of the block: the
+    // 16 threads of a half-warp then read 16 consecutive rows of a column
+    // (distinct banks with the 65-double row pitch)
+    const int tr = t >> 4, tc = t & 15;
     for (int j = 0; j < kNB; ++j) {
         if (t >= j && t < kNB) {
             double d = a[j][j];
@@ -328,18 +332,18 @@ __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, d
             else a[t][j] *= inv;
         }
         __syncthreads();
-        if (tr + 3 > j) {
+        if (tr + 48 > j) {
             double ci[4], cl[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                ci[u] = a[tr + u][j];
-                cl[u] = a[tc + u][j];
+                ci[u] = a[tr + 16 * u][j];
+                cl[u] = a[tc + 16 * u][j];
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u)
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
-                    const int i = tr + u, l = tc + v;
+                    const int i = tr + 16 * u, l = tc + 16 * v;
                     if (l > j && i >= l) a[i][l] -= ci[u] * cl[v];
                 }
         }
@@ -367,6 +371,7 @@ __device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double 
     const int nbk = min(kNB, m - r0);
     const int nbi = row_block_rows(ib, nblk, m);
     __syncthreads();
+#pragma unroll 4
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
         L[r][c] = (r < nbk && c < nbk) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
@@ -424,20 +429,22 @@ __device__ void syrk_tile(double *__restrict__ A, int m, int kb, long long t, do
     const int r0 = kb * kNB, i0 = row_block_start(ib, nblk, m), j0 = jb * kNB;
     const int nbk = min(kNB, m - r0), nbi = row_block_rows(ib, nblk, m), nbj = min(kNB, m - j0);
     __syncthreads();
+#pragma unroll 4
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
         Li[r][c] = (r < nbi && c < nbk) ? __ldcg(&A[(size_t)(i0 + r) * m + r0 + c]) : 0.0;
         Lj[r][c] = (r < nbj && c < nbk) ? __ldcg(&A[(size_t)(j0 + r) * m + r0 + c]) : 0.0;
     }
     __syncthreads();
-    const int tr = (threadIdx.x / 16) * 4, tc = (threadIdx.x % 16) * 4;
+    // rows tr + 16u, columns tc + 16v (conflict-free reads of Lj, see potrf_tile)
+    const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
     double acc[4][4] = {};
     for (int p = 0; p < nbk; ++p) {
         double a[4], b[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            a[u] = Li[tr + u][p];
-            b[u] = Lj[tc + u][p];
+            a[u] = Li[tr + 16 * u][p];
+            b[u] = Lj[tc + 16 * u][p];
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
@@ -448,7 +455,7 @@ __device__ void syrk_tile(double *__restrict__ A, int m, int kb, long long t, do
     for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            int r = tr + u, c = tc + v;
+            int r = tr + 16 * u, c = tc + 16 * v;
             if (r < nbi && c < nbj && (ib != jb || c <= r)) {
                 double *dst = &A[(size_t)(i0 + r) * m + j0 + c];
                 *dst = __ldcg(dst) - acc[u][v];
@@ -465,6 +472,7 @@ __device__ void bwd_diag(const double *__restrict__ A, int m, int kb, double *__
     double *dinv = sm + kNB * (kNB + 1);
     const int r0 = kb * kNB, nb = min(kNB, m - r0);
     __syncthreads();
+#pragma unroll 4
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         const int r = e / kNB, c = e % kNB;
         D[r][c] = (r < nb && c <= r) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : 0.0;
