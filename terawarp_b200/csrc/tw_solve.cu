@@ -504,15 +504,22 @@ __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict
     extern __shared__ double sm[];
     unsigned int gen = 0;
     const int nblk = (m + kNB - 1) / kNB;
+    if (blockIdx.x == 0) potrf_tile(A, m, 0, status, sm);
+    if (!grid_sync(bar, gen, status)) return;
     for (int kb = 0; kb < nblk; ++kb) {
-        if (blockIdx.x == 0) potrf_tile(A, m, kb, status, sm);
-        if (!grid_sync(bar, gen, status)) return;
         const int rest = nblk - kb - 1;
         // row blocks below the diagonal: the rest of A plus the right-hand-side block
         for (int b = blockIdx.x; b < rest + 1; b += gridDim.x) trsm_tile(A, m, kb, kb + 1 + b, sm);
         if (!grid_sync(bar, gen, status)) return;
+        // Lookahead: tile 0 of the trailing update is the next diagonal block
+        // (kb+1, kb+1), which no other tile of this step touches; CTA 0 updates
+        // it first and factors it at once, while the other CTAs are still on
+        // their tiles, so the next step needs no potrf phase of its own.
         const long long pairs = (long long)(rest + 1) * (rest + 2) / 2;
-        for (long long t = blockIdx.x; t < pairs; t += gridDim.x) syrk_tile(A, m, kb, t, sm);
+        for (long long t = blockIdx.x; t < pairs; t += gridDim.x) {
+            syrk_tile(A, m, kb, t, sm);
+            if (t == 0 && rest > 0) potrf_tile(A, m, kb + 1, status, sm);
+        }
         if (!grid_sync(bar, gen, status)) return;
     }
     // y' sits in rows m..m+3; back substitution L' x = y into Z rows 4..n-1

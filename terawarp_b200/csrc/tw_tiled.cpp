@@ -95,8 +95,15 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
             if (opts->tile[a] > 0) T[a] = opts->tile[a];
         if (opts->staging_depth > 0) depth = std::min(4, std::max(2, opts->staging_depth));
     }
-    if (kind == 1)  // TPS tiles start on control-cell boundaries
-        for (int a = 0; a < 3; ++a) T[a] = std::max<int64_t>(g, (T[a] / g) * g);
+    if (kind == 1) {
+        // TPS tiles start on resample-brick boundaries of the whole volume
+        // (256 in x, max(g, 8) in y, a control cell in z): every brick then has
+        // the origin it has in a whole-volume warp, so the tiled output equals
+        // the whole-volume output voxel for voxel
+        int64_t bd[3];
+        brick_dims(1, g, bd);
+        for (int a = 0; a < 3; ++a) T[a] = std::max<int64_t>(bd[a], (T[a] / bd[a]) * bd[a]);
+    }
     for (int a = 0; a < 3; ++a) T[a] = std::min(T[a], out_sz[a]);
     int64_t nt[3];
     for (int a = 0; a < 3; ++a) nt[a] = (out_sz[a] + T[a] - 1) / T[a];

@@ -99,3 +99,20 @@ def test_tiled_affine_matches_device_path(ctx, out_shape):
     torch.cuda.synchronize()
     agree(out, dst.cpu().numpy())
     agree(out, O.affine_warp(img, M, out_shape))
+
+
+def test_autotuned_tile_choice_gives_the_whole_volume_result(ctx):
+    """The autotuner times real tiled runs on the corner block; whatever it
+    picks, the tiled warp equals the whole-volume warp."""
+    from terawarp_b200 import autotune
+    shape = (40, 96, 136)
+    rng = np.random.default_rng(21)
+    vol = rng.integers(0, 4096, size=shape).astype(np.uint16)
+    sub, tar = synth.lattice_landmarks(shape[::-1], 40, 22, margin=6.0)
+    cands = [((64, 64, 32), 2), ((32, 32, 16), 3), ((128, 96, 40), 2)]
+    tile, depth, table = autotune.tune_tiled_tps(ctx, sub, tar, 1.0, 8, vol, sample_zyx=(32, 64, 96),
+                                                 candidates=cands)
+    assert (tile, depth) in [(t, d) for t, d in cands] and len(table) == 3
+    tiled = api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, 8, vol, tile=tile, depth=depth)
+    whole = tw.imgwarp_smallmemory_image(ctx, sub, tar, 8, 8, 8, 1, 0, vol)
+    np.testing.assert_array_equal(tiled, whole)
