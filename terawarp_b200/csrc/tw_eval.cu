@@ -9,12 +9,15 @@
 // coefficients) are staged through shared memory in tiles and read as
 // warp-wide broadcasts; each thread evaluates kNPT nodes so every shared
 // load feeds kNPT node-landmark pairs.  Per pair: 3 FADD, 1 FMUL, 2 FFMA,
-// 1 sqrt, 3 FFMA.  Sums are two-level: plain FP32 FMA chains over 32
-// landmarks, then Kahan-compensated accumulation of those partials.
+// 1 sqrt, 3 FFMA, issued as Blackwell FP32x2 instructions over two nodes at a
+// time (the landmark is staged with each component duplicated, negated
+// centre), so a pair costs ~5.5 issue slots.  Sums are two-level: plain FP32
+// FMA chains over 32 landmarks, then Kahan-compensated accumulation of those
+// partials.
 //
 // Coordinates are taken relative to an origin o near the landmarks so the
-// FP32 magnitudes stay small; the affine part is pre-folded on the host in
-// FP64 into a0 + alin * p' with the identity already subtracted, so the
+// FP32 magnitudes stay small; the affine part is folded (in FP64, on the
+// device) into a0 + alin * p' with the identity already subtracted, so the
 // kernel writes the displacement f(p) - p directly without cancelling two
 // large numbers.
 
@@ -46,8 +49,8 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
 
 __global__ void __launch_bounds__(kEvalThreads) k_tps_eval(EvalParams p)
 {
-    __shared__ float4 s_ctr[kTile];
-    __shared__ float4 s_coef[kTile];
+    // per landmark: (-cx, -cx, -cy, -cy), (-cz, -cz, wx, wx), (wy, wy, wz, wz)
+    __shared__ float4 s_lm[kTile][3];
     const int64_t nnodes = p.gsz[0] * p.gsz[1] * p.gsz[2];
     const int64_t base = (int64_t)blockIdx.x * (kEvalThreads * kNPT) + threadIdx.x;
 
@@ -68,43 +71,60 @@ __global__ void __launch_bounds__(kEvalThreads) k_tps_eval(EvalParams p)
         cx[j] = cy[j] = cz[j] = 0.f;
     }
 
+    float2 px2[kNPT / 2], py2[kNPT / 2], pz2[kNPT / 2];
+#pragma unroll
+    for (int k = 0; k < kNPT / 2; ++k) {
+        px2[k] = make_float2(px[2 * k], px[2 * k + 1]);
+        py2[k] = make_float2(py[2 * k], py[2 * k + 1]);
+        pz2[k] = make_float2(pz[2 * k], pz[2 * k + 1]);
+    }
+
     for (int t0 = 0; t0 < p.n; t0 += kTile) {
         const int cnt = min(kTile, p.n - t0);
         __syncthreads();
         for (int l = threadIdx.x; l < kTile; l += kEvalThreads) {
+            float4 c = make_float4(0.f, 0.f, 0.f, 0.f), w = c;  // zero weight pads the tile
             if (l < cnt) {
-                s_ctr[l] = p.ctr[t0 + l];
-                s_coef[l] = p.coef[t0 + l];
-            } else {
-                s_ctr[l] = make_float4(0.f, 0.f, 0.f, 0.f);
-                s_coef[l] = make_float4(0.f, 0.f, 0.f, 0.f);  // zero weight pads the tile
+                c = p.ctr[t0 + l];
+                w = p.coef[t0 + l];
             }
+            s_lm[l][0] = make_float4(-c.x, -c.x, -c.y, -c.y);
+            s_lm[l][1] = make_float4(-c.z, -c.z, w.x, w.x);
+            s_lm[l][2] = make_float4(w.y, w.y, w.z, w.z);
         }
         __syncthreads();
         const int nsub = (cnt + kSub - 1) / kSub;
         for (int sb = 0; sb < nsub; ++sb) {
-            float ax[kNPT], ay[kNPT], az[kNPT];
+            // node pairs (2k, 2k+1); the same operations, in the same order,
+            // as one FP32 instruction per node and landmark
+            float2 ax[kNPT / 2], ay[kNPT / 2], az[kNPT / 2];
 #pragma unroll
-            for (int j = 0; j < kNPT; ++j) ax[j] = ay[j] = az[j] = 0.f;
+            for (int k = 0; k < kNPT / 2; ++k) ax[k] = ay[k] = az[k] = make_float2(0.f, 0.f);
 #pragma unroll 4
             for (int l = sb * kSub; l < sb * kSub + kSub; ++l) {
-                const float4 c = s_ctr[l];
-                const float4 w = s_coef[l];
+                const float4 A = s_lm[l][0], B = s_lm[l][1], Cw = s_lm[l][2];
+                const float2 ncx = make_float2(A.x, A.y), ncy = make_float2(A.z, A.w);
+                const float2 ncz = make_float2(B.x, B.y), wx = make_float2(B.z, B.w);
+                const float2 wy = make_float2(Cw.x, Cw.y), wz = make_float2(Cw.z, Cw.w);
 #pragma unroll
-                for (int j = 0; j < kNPT; ++j) {
-                    float dx = px[j] - c.x, dy = py[j] - c.y, dz = pz[j] - c.z;
-                    float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    float r = fast_sqrt(r2);
-                    ax[j] = fmaf(r, w.x, ax[j]);
-                    ay[j] = fmaf(r, w.y, ay[j]);
-                    az[j] = fmaf(r, w.z, az[j]);
+                for (int k = 0; k < kNPT / 2; ++k) {
+                    const float2 dx = __fadd2_rn(px2[k], ncx), dy = __fadd2_rn(py2[k], ncy);
+                    const float2 dz = __fadd2_rn(pz2[k], ncz);
+                    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                    const float2 r = make_float2(fast_sqrt(r2.x), fast_sqrt(r2.y));
+                    ax[k] = __ffma2_rn(r, wx, ax[k]);
+                    ay[k] = __ffma2_rn(r, wy, ay[k]);
+                    az[k] = __ffma2_rn(r, wz, az[k]);
                 }
             }
 #pragma unroll
             for (int j = 0; j < kNPT; ++j) {
-                kahan_add(sx[j], cx[j], ax[j]);
-                kahan_add(sy[j], cy[j], ay[j]);
-                kahan_add(sz[j], cz[j], az[j]);
+                const float axj = (j & 1) ? ax[j >> 1].y : ax[j >> 1].x;
+                const float ayj = (j & 1) ? ay[j >> 1].y : ay[j >> 1].x;
+                const float azj = (j & 1) ? az[j >> 1].y : az[j >> 1].x;
+                kahan_add(sx[j], cx[j], axj);
+                kahan_add(sy[j], cy[j], ayj);
+                kahan_add(sz[j], cz[j], azj);
             }
         }
     }
