@@ -635,8 +635,7 @@ __device__ __forceinline__ void tps_pair(const float4 *Q, const BrickCtx<T> &B, 
     using Gm = Geom<G>;
     const float4 *qn = Q + y * Gm::NX + x / G;
     const float4 n0 = qn[0], n1 = qn[1], n2 = qn[2], n3 = qn[3];
-    uint32_t outv[2];
-    if (INTERP == 0) {
+    if constexpr (INTERP == 0) {
         const float4 n[4] = {n0, n1, n2, n3};
         float2 p0, p1, pz2;
         pair_positions(n, B.pw, p0, p1, pz2);
@@ -654,24 +653,26 @@ __device__ __forceinline__ void tps_pair(const float4 *Q, const BrickCtx<T> &B, 
                 pair_checked2<T, true, int64_t>(p0, p1, pz2, B.base, B.py, B.pz, B.frame, B.cw.cl, B.cw.ch, nv, w);
             store_packed<T>(drow + x, w, B.pair_ok, nv);
         }
-        return;
-    }
+    } else {
+        uint32_t outv[2];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const float4 w = B.wx[j];
-        const float qx = fmaf(w.x, n0.x, fmaf(w.y, n1.x, fmaf(w.z, n2.x, w.w * n3.x)));
-        const float qy = fmaf(w.x, n0.y, fmaf(w.y, n1.y, fmaf(w.z, n2.y, w.w * n3.y)));
-        const float qz = fmaf(w.x, n0.z, fmaf(w.y, n1.z, fmaf(w.z, n2.z, w.w * n3.z)));
-        float v;
-        if (fast) {
-            v = sample_fast<T, INTERP>(B.base, B.py32, B.pz32, qx, qy, qz);
-            outv[j] = INTERP == 1 ? (uint32_t)v : to_out<T, true>(v);
-        } else {
-            const bool ok = (x + j) < B.xe && sample_checked<T, INTERP>(B.base, B.py, B.pz, B.frame, qx, qy, qz, v);
-            outv[j] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, true>(v)) : 0u;
+        for (int j = 0; j < 2; ++j) {
+            const float4 w = B.wx[j];
+            const float qx = fmaf(w.x, n0.x, fmaf(w.y, n1.x, fmaf(w.z, n2.x, w.w * n3.x)));
+            const float qy = fmaf(w.x, n0.y, fmaf(w.y, n1.y, fmaf(w.z, n2.y, w.w * n3.y)));
+            const float qz = fmaf(w.x, n0.z, fmaf(w.y, n1.z, fmaf(w.z, n2.z, w.w * n3.z)));
+            float v;
+            if (fast) {
+                v = sample_fast<T, INTERP>(B.base, B.py32, B.pz32, qx, qy, qz);
+                outv[j] = INTERP == 1 ? (uint32_t)v : to_out<T, true>(v);
+            } else {
+                const bool ok =
+                    (x + j) < B.xe && sample_checked<T, INTERP>(B.base, B.py, B.pz, B.frame, qx, qy, qz, v);
+                outv[j] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, true>(v)) : 0u;
+            }
         }
+        store_pair<T>(drow + x, outv[0], outv[1], B.pair_ok, fast ? 2 : B.xe - x);
     }
-    store_pair<T>(drow + x, outv[0], outv[1], B.pair_ok, fast ? 2 : B.xe - x);
 }
 
 // ALL_FAST: the whole slice is inside; else segf[y*4 + k] says whether the
@@ -892,8 +893,7 @@ __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float 
         for (int k = 0; k < kBX / 64; ++k) {
             const int x = 2 * lane + 64 * k;
             if (!FAST && x >= xe) continue;
-            uint32_t outv[2];
-            if (INTERP == 0) {  // packed pair path, truncation (no +0.5)
+            if constexpr (INTERP == 0) {  // packed pair path, truncation (no +0.5)
                 const float lx = (float)x;
                 const float2 p0 = f2(fmaf(m[0][0], lx, bx0), fmaf(m[1][0], lx, by0));
                 const float2 p1 = add2(p0, f2(m[0][0], m[1][0]));
@@ -909,22 +909,23 @@ __device__ __forceinline__ void affine_rows(const float (&m)[3][3], const float 
                 else
                     pair_checked2<T, false, int64_t>(p0, p1, pz2, base, py, pz, frame, cw.cl, cw.ch, xe - x, w);
                 store_packed<T>(drow + x, w, pair_ok, FAST ? 2 : xe - x);
-                continue;
-            }
+            } else {
+                uint32_t outv[2];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const float lx = (float)(x + j);
-                const float qx = fmaf(m[0][0], lx, bx0), qy = fmaf(m[1][0], lx, by0), qz = fmaf(m[2][0], lx, bz0);
-                float v;
-                if (FAST) {
-                    v = sample_fast<T, INTERP>(base, py32, pz32, qx, qy, qz);
-                    outv[j] = INTERP == 1 ? (uint32_t)v : to_out<T, false>(v);
-                } else {
-                    const bool ok = (x + j) < xe && sample_checked<T, INTERP>(base, py, pz, frame, qx, qy, qz, v);
-                    outv[j] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, false>(v)) : 0u;
+                for (int j = 0; j < 2; ++j) {
+                    const float lx = (float)(x + j);
+                    const float qx = fmaf(m[0][0], lx, bx0), qy = fmaf(m[1][0], lx, by0), qz = fmaf(m[2][0], lx, bz0);
+                    float v;
+                    if (FAST) {
+                        v = sample_fast<T, INTERP>(base, py32, pz32, qx, qy, qz);
+                        outv[j] = INTERP == 1 ? (uint32_t)v : to_out<T, false>(v);
+                    } else {
+                        const bool ok = (x + j) < xe && sample_checked<T, INTERP>(base, py, pz, frame, qx, qy, qz, v);
+                        outv[j] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, false>(v)) : 0u;
+                    }
                 }
+                store_pair<T>(drow + x, outv[0], outv[1], pair_ok, FAST ? 2 : xe - x);
             }
-            store_pair<T>(drow + x, outv[0], outv[1], pair_ok, FAST ? 2 : xe - x);
         }
     }
 }
