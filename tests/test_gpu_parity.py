@@ -43,7 +43,9 @@ def vol(shape_zyx, dtype, seed):
 
 # ------------------------------------------------------------------ solve
 
-@pytest.mark.parametrize("n", [4, 5, 16, 64, 300, 1000])
+# 68 and 132: the projected matrix fills exactly one / two 64-blocks, so the
+# right-hand-side rows form a row block of their own right after a full block
+@pytest.mark.parametrize("n", [4, 5, 16, 64, 68, 132, 300, 1000, 2048])
 def test_solve_matches_oracle(ctx, n):
     sub, tar = landmarks(n, (200, 180, 90), n)
     t = tw.tps_solve(ctx, sub, tar)
@@ -79,7 +81,7 @@ def test_solve_rejects_too_few_points(ctx):
 # ------------------------------------------------------------- node grid
 
 @pytest.mark.parametrize("g,n,sz", [(4, 12, (36, 30, 22)), (8, 64, (256, 256, 128)), (16, 500, (512, 512, 256)),
-                                    (16, 2000, (1024, 1024, 512))])
+                                    (16, 2000, (1024, 1024, 512)), (8, 2000, (1024, 1024, 256))])
 def test_grid_eval_error_below_hundredth_voxel(ctx, g, n, sz):
     if n >= 500:
         sub, tar = synth.lattice_landmarks(sz, n, 11)
