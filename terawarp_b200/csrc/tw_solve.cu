@@ -244,9 +244,12 @@ __global__ void k_fill_a(const double *__restrict__ ctr, int n, const double *__
 
 constexpr int kSolveThreads = 256;
 constexpr int kStTimeout = 4;
-// a CTA gives up on a barrier after this long (ns); the launch is cooperative
-// so every CTA is resident, and the wait is bounded all the same
-constexpr unsigned long long kBarrierLimitNs = 5000000000ull;
+// A CTA gives up on a barrier after this long (ns).  The launch is
+// cooperative, so every CTA can be resident at once; while other work (the
+// previous job's resample, a caller's kernel on another stream) still holds
+// SMs, some CTAs start later than others and the early ones wait, so the
+// bound is generous, but it is a bound.
+constexpr unsigned long long kBarrierLimitNs = 30000000000ull;
 
 struct GridBar {
     unsigned int count;   // CTAs arrived at the current barrier
