@@ -228,7 +228,10 @@ int tw_box_writer_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t n
                        const void *src);
 
 typedef struct {
-    int64_t tile[3];        /* output tile dims (0 = 512^3; reference: 1000^3)  */
+    int64_t tile[3];        /* output tile dims x, y, z (0 = 512; reference:    */
+                            /* 1000^3); TPS tiles are rounded down to whole     */
+                            /* resample bricks (256 x max(g,8) x g), at least   */
+                            /* one brick                                        */
     int staging_depth;      /* tiles in flight, 2..4 (0 = 2: double buffering)  */
     int interp;             /* tw_interp                                        */
 } tw_tile_opts;
@@ -238,7 +241,8 @@ typedef struct {
  * node grid device-resident, and streams output tiles through pinned
  * double-buffered transfers on separate copy/compute streams.  Each tile's
  * source box is the exact footprint of its samples (convex-hull bound of the
- * B-spline), so the tiled result equals the whole-volume result.
+ * B-spline) and tiles start on the whole volume's brick boundaries, so the
+ * tiled result equals the whole-volume result voxel for voxel.
  * marker_scale multiplies both marker sets (the reference uses 4 for markers
  * placed on a 4x downsampled image, :1194-1203). */
 tw_status tw_imgwarp_smallmemory_tiled(tw_ctx *ctx, const tw_marker *ql_marker_tar,
