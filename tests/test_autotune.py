@@ -44,3 +44,15 @@ def test_cache_round_trip(tmp_path):
     data = json.loads(p.read_text())
     assert data["k"]["tile"] == [512, 512, 512] and data["k"]["depth"] == 2
     assert data["k2"]["table"][1] == [[1024, 1024, 256], 3, 0.25]
+
+
+def test_tune_tiled_tps_returns_a_cached_choice_without_running(tmp_path):
+    import numpy as np
+    src = np.zeros((64, 128, 256), np.uint16)
+    tar = np.zeros((100, 3), np.float32)
+    key = autotune.cache_key("tps", src.shape, "u16", 16, 100, "B200")
+    path = tmp_path / "a.json"
+    autotune.store_cache(path, key, (256, 128, 64), 3, [((256, 128, 64), 3, 0.01)])
+    tile, depth, table = autotune.tune_tiled_tps(None, tar, tar, 1.0, 16, src, cache_path=path, device_name="B200")
+    assert (tile, depth) == ((256, 128, 64), 3)
+    assert table == [((256, 128, 64), 3, 0.01)]
