@@ -13,7 +13,13 @@ FP32 compensated node evaluation, fused B-spline + trilinear resample.
   roofline  the resample kernel: algorithmic bytes (2 x 2 B per voxel + 12 B
           per node) / its measured duration vs MEASURED_PEAKS.json hbm_gbs
   cpu_baseline  the FP64 oracle (a restatement of the reference's CPU path)
-          on a bounded slab of the same job, extrapolated, all host threads
+          on the same inputs: solve and the whole node grid timed in full, the
+          warp timed on the first 16-plane cell layer and scaled by the number
+          of layers; all host threads, and (under "serial") one thread, the
+          reference's own threading of the whole-image path
+  accuracy  node displacement max / RMS against the FP64 oracle over the
+          whole grid at spacing 8 and 16, and the share of output voxels
+          within +-1 level on two 512^3 tiles of the measured output
   serving the serving mix (Poisson arrivals, mixed affine/rigid/TPS jobs of
           uneven sizes) through the continuous-batching server: p50/p99 job
           latency and aggregate GVoxel/s, capacity with every job submitted at
@@ -60,6 +66,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-affine", action="store_true", help="skip the affine leg")
     ap.add_argument("--no-tiled", action="store_true", help="skip the tiled (out-of-core) leg")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the error figures against the FP64 oracle")
     ap.add_argument("--serve-jobs", type=int, default=32, help="jobs in the serving leg")
     ap.add_argument("--small", action="store_true", help="256x256x128 case, 64 landmarks")
     ap.add_argument("--shape", type=str, default="", help="X,Y,Z volume for profiling captures (default: full)")
@@ -168,57 +175,109 @@ def barrier(ws: int):
 
 # ----------------------------------------------------------------- CPU legs
 
-def cpu_reference_rate(vol_zyx_slab, sub, tar, full_planes: int, threads: int = 0):
-    """FP64 oracle on a slab of output planes; extrapolates the job time to the
-    full volume (solve once + per-plane grid and warp).  Returns (GVoxel/s,
-    seconds of CPU work, description)."""
+SLAB_PLANES = G        # one whole cell layer: the oracle expands whole cells
+
+
+def oracle_solve_grid(sub, tar, Z, threads):
+    """FP64 oracle solve and whole node grid, each timed in full (their cost
+    does not depend on the output planes).  Returns (c, d, grid, solve s, grid s,
+    planes the first cell layer's samples can read)."""
+    import numpy as np
+
     from oracle import oracle as O
-    slab = vol_zyx_slab
-    Z, Y, X = slab.shape
+    X, Y = SHAPE_ZYX[2], SHAPE_ZYX[1]
     t0 = time.perf_counter()
     c, d = O.tps_solve(tar, sub, 0.2, threads)
     t1 = time.perf_counter()
     gsz = (O.grid_size(X, G), O.grid_size(Y, G), O.grid_size(Z, G))
     df = O.tps_grid(tar, c, d, gsz, G, threads=threads)
     t2 = time.perf_counter()
-    O.tps_warp(slab, df, G, 0, threads)
-    t3 = time.perf_counter()
-    per_plane = ((t2 - t1) + (t3 - t2)) / Z
-    job = (t1 - t0) + per_plane * full_planes
-    vox = X * Y * full_planes
-    desc = (f"FP64 oracle (restatement of the reference CPU path), solve n={len(sub)} in full + grid/warp of a "
-            f"{X}x{Y}x{Z} slab, extrapolated to {full_planes} planes")
-    return vox / job / 1e9, t3 - t0, desc
+    # the first cell layer's samples are convex combinations of node planes
+    # 0..3 (B-spline weights >= 0, sum 1): q_z <= zmax, taps read planes up to
+    # floor(zmax) + 1; two planes of margin on top
+    zpos = (np.arange(4) - 1) * G
+    zmax = float((df[:4, :, :, 2] + zpos[:, None, None]).max())
+    need = int(min(Z, max(SLAB_PLANES, np.ceil(zmax) + 4)))
+    return c, d, df, t1 - t0, t2 - t1, need
+
+
+def cpu_slab_warp(planes, df, Z, threads, repeats=1):
+    """Seconds of the oracle's warp of the first cell layer (SLAB_PLANES output
+    planes, per-cell B-spline expansion included), median of `repeats`."""
+    from oracle import oracle as O
+    X, Y = SHAPE_ZYX[2], SHAPE_ZYX[1]
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        O.tps_warp_box(planes, df, G, (0, 0, 0), (X, Y, SLAB_PLANES), 0, threads, planes_of=Z)
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times)
+
+
+def cpu_baseline_figures(planes_fn, sub, tar, Z):
+    """The FP64 oracle on the benchmark's own inputs, with the reference's
+    whole-image threading (serial: no OpenMP in the grid loop or the block
+    warp, q_imgwarp_tps_quicksmallmemory.cpp:620-648, :2121-2133) and with all
+    host threads (OpenMP).  Solve and node grid are timed in full; the warp is
+    timed on the first cell layer and scaled by Z / SLAB_PLANES (its cost is
+    the same per cell layer).  planes_fn(k) returns the volume's first k
+    planes as a (k, Y, X) array."""
+    from oracle import oracle as O
+    X, Y = SHAPE_ZYX[2], SHAPE_ZYX[1]
+    out = {}
+    planes = None
+    for label, threads in (("omp", O.max_threads()), ("serial", 1)):
+        c, d, df, ts, tg, need = oracle_solve_grid(sub, tar, Z, threads)
+        if planes is None or planes.shape[0] < need:
+            planes = planes_fn(need)
+        slab = cpu_slab_warp(planes, df, Z, threads)
+        job = ts + tg + slab * (Z / SLAB_PLANES)
+        out[label] = {"value": X * Y * Z / job / 1e9, "threads": threads, "job_s": job, "solve_s": ts,
+                      "grid_s": tg, "slab_warp_s": slab}
+    return out
+
+
+def cpu_sample_text(fig):
+    return (f"FP64 oracle (restatement of the reference CPU path) on the benchmark's own inputs: solve "
+            f"(n={N_LANDMARKS}) and the whole g={G} node grid timed in full; warp timed on the first "
+            f"{SLAB_PLANES}-plane cell layer of the {SHAPE_ZYX[2]}x{SHAPE_ZYX[1]} volume and scaled by "
+            f"{SHAPE_ZYX[0] // SLAB_PLANES} layers; {fig['threads']} thread(s)")
 
 
 def run_reference(args):
-    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference arm: the FP64 oracle restatement of the reference's CPU
+    path on all host threads, on the same workload and inputs as our arm
+    (landmarks and volume planes from the same seed).  Solve and node grid are
+    timed once in full; each step warps the first cell layer; the job time is
+    solve + grid + layers x median layer time.  Rank 0 alone runs it."""
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import numpy as np
-    import torch
-
     from oracle import oracle as O
     from terawarp_b200 import synth
     threads = O.max_threads()
-    slab_planes = 8
-    case = synth.large_tps_case(SEED, "cpu", shape_zyx=(slab_planes, SHAPE_ZYX[1], SHAPE_ZYX[2]), n=N_LANDMARKS,
-                                g=G, n_blobs=2000, n_fibres=200)
-    sub, tar = synth.lattice_landmarks((SHAPE_ZYX[2], SHAPE_ZYX[1], SHAPE_ZYX[0]), N_LANDMARKS, SEED + 7)
-    slab = case.vol.numpy()
-    rates = []
-    for i in range(args.warmup + args.steps):
-        r, secs, desc = cpu_reference_rate(slab, sub, tar, SHAPE_ZYX[0], threads)
-        if i >= args.warmup:
-            rates.append(r)
-    v = statistics.median(rates)
-    ms = SHAPE_ZYX[0] * SHAPE_ZYX[1] * SHAPE_ZYX[2] / (v * 1e9) * 1e3
+    Z, Y, X = SHAPE_ZYX
+    lm = synth.large_tps_case(SEED, "cpu", shape_zyx=SHAPE_ZYX, n=N_LANDMARKS, g=G, z_range=(0, 1))
+    sub, tar = lm.marker_sub, lm.marker_tar
+    if args.warmup > 0:
+        oracle_solve_grid(sub, tar, Z, threads)
+    c, d, df, ts, tg, need = oracle_solve_grid(sub, tar, Z, threads)
+    planes = synth.large_tps_case(SEED, "cpu", shape_zyx=SHAPE_ZYX, n=N_LANDMARKS, g=G,
+                                  z_range=(0, need)).vol.numpy()
+    for _ in range(args.warmup):
+        cpu_slab_warp(planes, df, Z, threads)
+    slabs = [cpu_slab_warp(planes, df, Z, threads) for _ in range(args.steps)]
+    job = ts + tg + statistics.median(slabs) * (Z / SLAB_PLANES)
+    v = X * Y * Z / job / 1e9
+    fig = {"threads": threads}
     line = {"metric": METRIC, "value": v, "unit": "GVoxel/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": job * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "volume_xyz": [SHAPE_ZYX[2], SHAPE_ZYX[1], SHAPE_ZYX[0]],
-                       "landmarks": N_LANDMARKS, "grid_spacing": G, "interp": "trilinear"},
-            "cpu_baseline": {"value": v, "unit": "GVoxel/s", "cores": threads, "kind": "port", "sample": desc},
+            "config": {"workload": WORKLOAD, "volume_xyz": [X, Y, Z], "landmarks": N_LANDMARKS, "grid_spacing": G,
+                       "interp": "trilinear"},
+            "cpu_baseline": {"value": v, "unit": "GVoxel/s", "cores": threads, "kind": "port",
+                             "sample": cpu_sample_text(fig), "solve_s": ts, "grid_s": tg,
+                             "slab_warp_s": [round(x, 4) for x in slabs]},
             "e2e": {"value": v, "unit": "GVoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -375,6 +434,58 @@ def serving_leg(ctx, device: int, n_jobs: int, seed: int = 1239, rate_hz: float 
     }
 
 
+# ----------------------------------------------------------- accuracy
+
+def accuracy_leg(ctx, case, dst, tile: int = 512):
+    """Errors of the benchmark job against the FP64 oracle: node displacement
+    max / RMS (voxels) over the whole control grid at spacing 8 and 16, and
+    the share of output voxels within +-1 level (and exact) on two tile^3
+    boxes -- the corner tile and a seeded interior one -- of the measured
+    g = 16 output `dst`, the oracle using its own FP64 solve and node grid."""
+    import numpy as np
+    import torch
+
+    import terawarp_b200 as tw
+    from oracle import oracle as O
+
+    Z, Y, X = case.vol.shape
+    tar, sub = case.marker_tar, case.marker_sub
+    c, d = O.tps_solve(tar, sub)
+    out = {}
+    for g in (8, 16):
+        gsz = (tw.grid_size(X, g), tw.grid_size(Y, g), tw.grid_size(Z, g))
+        t = tw.tps_solve(ctx, tar, sub)
+        nodes = tw.tps_eval_grid(ctx, t, gsz, g)
+        torch.cuda.synchronize()
+        t.close()
+        ref = O.tps_grid(tar, c, d, gsz, g)
+        err = np.abs(nodes[..., :3].cpu().numpy().astype(np.float64) - ref.astype(np.float64))
+        del nodes
+        out[f"g{g}"] = {"nodes": int(err.size // 3), "node_max_err_vox": float(err.max()),
+                        "node_rms_err_vox": float(np.sqrt((err ** 2).mean()))}
+        if g != 16:
+            continue
+        src_h = case.vol.cpu().numpy()
+        rng = np.random.default_rng(2024)
+        t = min(tile, X, Y, Z)
+        boxes = [(0, 0, 0), tuple(int(v) for v in rng.integers(0, [X - t + 1, Y - t + 1, Z - t + 1]))]
+        n_in = n_ex = n = 0
+        dmax = 0
+        for (x0, y0, z0) in boxes:
+            r = O.tps_warp_box(src_h, ref, g, (x0, y0, z0), (t, t, t))
+            got = dst[z0:z0 + t, y0:y0 + t, x0:x0 + t].cpu().numpy()
+            dd = np.abs(got.astype(np.int64) - r.astype(np.int64))
+            n_in += int((dd <= 1).sum())
+            n_ex += int((dd == 0).sum())
+            n += dd.size
+            dmax = max(dmax, int(dd.max()))
+        del src_h
+        out["intensity_g16"] = {"within1_frac": n_in / n, "exact_frac": n_ex / n, "max_diff": dmax, "voxels": n,
+                                "boxes_xyz": [list(b) for b in boxes], "box_edge": t}
+    out["reference"] = "FP64 oracle: solve, node grid (stored as float) and per-cell B-spline warp in double"
+    return out
+
+
 # ----------------------------------------------------------------- our arm
 
 def run_ours(args):
@@ -503,6 +614,8 @@ def run_ours(args):
         equal = bool(torch.equal(h_dst, dst.cpu()))
         line["e2e"]["matches_device_path"] = equal
         del h_src, h_dst
+    if rank == 0 and not args.no_accuracy:
+        line["accuracy"] = accuracy_leg(ctx, case, dst)
     if rank == 0 and not args.no_affine and not args.small and not args.shape:
         line["affine"] = affine_leg(ctx, local)
     if rank == 0 and not args.no_tiled and not args.small and not args.shape:
@@ -510,12 +623,14 @@ def run_ours(args):
     if rank == 0 and not args.no_serve and not args.small and not args.shape:
         line["serving"] = serving_leg(ctx, local, args.serve_jobs)
     if rank == 0 and ws == 1 and not args.no_cpu and not args.small and not args.shape:
-        from oracle import oracle as O
-        slab_planes = 8
-        slab = src[:slab_planes].cpu().numpy()
-        r, secs, desc = cpu_reference_rate(slab, sub, tar, Z, 0)
-        line["cpu_baseline"] = {"value": r, "unit": "GVoxel/s", "cores": O.max_threads(), "kind": "port",
-                                "sample": desc, "seconds": secs}
+        figs = cpu_baseline_figures(lambda k: src[:k].cpu().numpy(), sub, tar, Z)
+        omp, ser = figs["omp"], figs["serial"]
+        line["cpu_baseline"] = {"value": omp["value"], "unit": "GVoxel/s", "cores": omp["threads"], "kind": "port",
+                                "sample": cpu_sample_text(omp), "solve_s": omp["solve_s"], "grid_s": omp["grid_s"],
+                                "slab_warp_s": omp["slab_warp_s"],
+                                "serial": {"value": ser["value"], "unit": "GVoxel/s", "cores": 1,
+                                           "sample": cpu_sample_text(ser), "solve_s": ser["solve_s"],
+                                           "grid_s": ser["grid_s"], "slab_warp_s": ser["slab_warp_s"]}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

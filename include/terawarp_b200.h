@@ -140,10 +140,14 @@ tw_status tw_fit_affine(tw_ctx *ctx, const tw_marker *tar, const tw_marker *sub,
  * returns TW_ERR_ARG.
  * Same kernel, same FP64 arithmetic and same result as tw_fit_affine.
  * Calls that overlapped on the GPU would race on that one array, so calls for
- * the same device are serialised by a lock inside the library.  The first
- * call on each device looks up the array's address (and may load the device
- * code); make it before any stream capture begins.  Synchronises ctx's
- * stream. */
+ * the same device are serialised by a lock inside the library, which is held
+ * until ctx's stream has finished the call's work (on error returns too).
+ * The first call on each device looks up the array's address (and may load
+ * the device code); make it before any stream capture begins.  The lookup is
+ * repeated when the device's context was destroyed and created again since
+ * (cudaDeviceReset), because the array then lives at a new address.
+ * Synchronises ctx's stream; the caller's current device is unchanged on
+ * return. */
 tw_status tw_fit_affine_noalloc(tw_ctx *ctx, const tw_marker *tar, const tw_marker *sub, int n, double M[16]);
 
 /* Builds the pull-back matrix of the TeraWarp command's parameter surface

@@ -46,6 +46,10 @@ def load():
     lib.or_tps_warp.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_int64, C.c_int64, _f32p, C.c_int64, C.c_int64,
                                 C.c_int64, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.or_tps_warp.restype = C.c_int
+    lib.or_tps_warp_box.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_int64, C.c_int64, _f32p, C.c_int64,
+                                    C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64,
+                                    C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_void_p]
+    lib.or_tps_warp_box.restype = C.c_int
     lib.or_affine_fit.argtypes = [C.c_int, _f64p, _f64p, _f64p]
     lib.or_affine_fit.restype = C.c_int
     lib.or_affine_warp.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_int64, C.c_int64, _f64p, C.c_int, C.c_int,
@@ -100,6 +104,30 @@ def tps_warp(src: np.ndarray, df: np.ndarray, g: int, interp: int = 0, threads: 
                             interp, threads, out.ctypes.data)
     if rc != 0:
         raise RuntimeError(f"oracle tps_warp failed with {rc}")
+    return out
+
+
+def tps_warp_box(src: np.ndarray, df: np.ndarray, g: int, box_o_xyz, box_n_xyz, interp: int = 0,
+                 threads: int = 0, planes_of: int | None = None) -> np.ndarray:
+    """The whole-volume warp's output restricted to the box [o, o + n)
+    (x, y, z voxels): an (nz, ny, nx) array equal to that box of tps_warp's
+    result.  planes_of = Z says that src holds only the first planes of a
+    volume of Z planes (the range rule uses Z); the caller guarantees that the
+    box's samples read no plane beyond those given."""
+    src = np.ascontiguousarray(src)
+    Z, Y, X = src.shape
+    if planes_of is not None:
+        if planes_of < Z:
+            raise ValueError("planes_of must be at least the planes given")
+        Z = int(planes_of)
+    gz, gy, gx, _ = df.shape
+    ox, oy, oz = (int(v) for v in box_o_xyz)
+    nx, ny, nz = (int(v) for v in box_n_xyz)
+    out = np.zeros((nz, ny, nx), src.dtype)
+    rc = load().or_tps_warp_box(src.ctypes.data, _dt(src), X, Y, Z, np.ascontiguousarray(df, np.float32), gx, gy,
+                                gz, g, interp, threads, ox, oy, oz, nx, ny, nz, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle tps_warp_box failed with {rc}")
     return out
 
 

@@ -446,18 +446,34 @@ static inline void store_vox(void *dst, int dt, int64_t idx, double v)
  * src/dst are x-fastest volumes of sz0 x sz1 x sz2 (dt 1 = u8, 2 = u16).
  * df is the node grid from or_tps_grid.  threads: 1 = serial as the
  * reference's whole-image path, 0 = all cores, k = k threads. */
-int or_tps_warp(const void *src, int dt, int64_t sz0, int64_t sz1, int64_t sz2,
-                const float *df, int64_t gsz0, int64_t gsz1, int64_t gsz2, int g,
-                int interp, int threads, void *dst)
+/* The same warp restricted to the output box [b0, b0 + bn) (global voxel
+ * coordinates, inside the volume), written to dst as an x-fastest bn0 x bn1 x
+ * bn2 buffer.  Only the cells that overlap the box are expanded; every
+ * voxel's arithmetic is the whole-volume warp's, so a box of the whole-volume
+ * output is reproduced exactly.  Used to check large volumes on a sample of
+ * tiles, and to time the CPU path on a slab of planes. */
+int or_tps_warp_box(const void *src, int dt, int64_t sz0, int64_t sz1, int64_t sz2,
+                    const float *df, int64_t gsz0, int64_t gsz1, int64_t gsz2, int g,
+                    int interp, int threads, int64_t b0x, int64_t b0y, int64_t b0z,
+                    int64_t bnx, int64_t bny, int64_t bnz, void *dst)
 {
     if (!src || !dst || !df || (dt != 1 && dt != 2) || g < 1) return OR_ERR_ARG;
     if (gsz0 < 4 || gsz1 < 4 || gsz2 < 4) return OR_ERR_ARG;
+    if (b0x < 0 || b0y < 0 || b0z < 0 || bnx < 1 || bny < 1 || bnz < 1 || b0x + bnx > sz0 || b0y + bny > sz1 ||
+        b0z + bnz > sz2)
+        return OR_ERR_ARG;
     set_threads(threads);
     double *TB = (double *)malloc(sizeof(double) * 4 * (size_t)g);
     if (!TB) return OR_ERR_OOM;
     or_bspline_tb(g, TB);
-    const int64_t ncz = gsz2 - 3, ncy = gsz1 - 3, ncx = gsz0 - 3;
-    const int64_t ncells = ncz * ncy * ncx;
+    /* cells [cl, ch) that overlap the box, within s < gsz - 3 */
+    const int64_t clx = b0x / g, cly = b0y / g, clz = b0z / g;
+    int64_t chx = (b0x + bnx + g - 1) / g, chy = (b0y + bny + g - 1) / g, chz = (b0z + bnz + g - 1) / g;
+    if (chx > gsz0 - 3) chx = gsz0 - 3;
+    if (chy > gsz1 - 3) chy = gsz1 - 3;
+    if (chz > gsz2 - 3) chz = gsz2 - 3;
+    const int64_t ncz = chz - clz, ncy = chy - cly, ncx = chx - clx;
+    const int64_t ncells = ncz > 0 && ncy > 0 && ncx > 0 ? ncz * ncy * ncx : 0;
     int rc = OR_OK;
 #pragma omp parallel if (threads != 1)
     {
@@ -470,9 +486,9 @@ int or_tps_warp(const void *src, int dt, int64_t sz0, int64_t sz1, int64_t sz2,
 #pragma omp for schedule(dynamic, 4)
         for (int64_t cell = 0; cell < ncells; ++cell) {
             if (!blk) continue;
-            int64_t scz = cell / (ncy * ncx);
-            int64_t scy = (cell / ncx) % ncy;
-            int64_t scx = cell % ncx;
+            int64_t scz = clz + cell / (ncy * ncx);
+            int64_t scy = cly + (cell / ncx) % ncy;
+            int64_t scx = clx + cell % ncx;
             /* gather in (dep, col, row) = (z, x, y) order */
             int ind = 0;
             for (int64_t dep = scz; dep < scz + 4; ++dep)
@@ -513,12 +529,15 @@ int or_tps_warp(const void *src, int dt, int64_t sz0, int64_t sz1, int64_t sz2,
                     for (int x = 0; x < g; ++x) {
                         int64_t pw0 = start_x + x, pw1 = start_y + y, pw2 = start_z + z;
                         if (pw0 >= sz0 || pw1 >= sz1 || pw2 >= sz2) continue;
+                        if (pw0 < b0x || pw1 < b0y || pw2 < b0z || pw0 >= b0x + bnx || pw1 >= b0y + bny ||
+                            pw2 >= b0z + bnz)
+                            continue;
                         const float *o = blk + 3 * (size_t)((z * g + y) * g + x);
                         double q[3];
                         q[0] = pw0 + (double)o[0];
                         q[1] = pw1 + (double)o[1];
                         q[2] = pw2 + (double)o[2];
-                        int64_t oi = (pw2 * sz1 + pw1) * sz0 + pw0;
+                        int64_t oi = ((pw2 - b0z) * bny + (pw1 - b0y)) * bnx + (pw0 - b0x);
                         if (q[0] < 0 || q[0] > sz0 - 1 || q[1] < 0 || q[1] > sz1 - 1 || q[2] < 0 || q[2] > sz2 - 1) {
                             store_vox(dst, dt, oi, 0.0);
                             continue;
@@ -540,6 +559,15 @@ int or_tps_warp(const void *src, int dt, int64_t sz0, int64_t sz1, int64_t sz2,
     }
     free(TB);
     return rc;
+}
+
+/* The whole-volume warp described above: the box is the whole volume. */
+int or_tps_warp(const void *src, int dt, int64_t sz0, int64_t sz1, int64_t sz2,
+                const float *df, int64_t gsz0, int64_t gsz1, int64_t gsz2, int g,
+                int interp, int threads, void *dst)
+{
+    return or_tps_warp_box(src, dt, sz0, sz1, sz2, df, gsz0, gsz1, gsz2, g, interp, threads, 0, 0, 0, sz0, sz1,
+                           sz2, dst);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -86,6 +86,17 @@ def _sz3(x) -> "C.Array":
     return (C.c_int64 * 3)(s[0], s[1], s[2])
 
 
+def _pair_count(a, b, what: str) -> int:
+    """Number of landmark pairs of two (n, 3) point sets; the C side reads n
+    points from both arrays, so a shorter second set would be read past its
+    end."""
+    na = len(np.asarray(a, dtype=np.float64).reshape(-1, 3))
+    nb = len(np.asarray(b, dtype=np.float64).reshape(-1, 3))
+    if na != nb:
+        raise ValueError(f"{what}: the two landmark sets differ in length ({na} vs {nb})")
+    return na
+
+
 def _markers(pts) -> "C.Array":
     a = np.ascontiguousarray(np.asarray(pts, dtype=np.float32).reshape(-1, 3))
     if len(a) == 0:
@@ -166,9 +177,9 @@ class TPS:
 
 def tps_solve(ctx: Context, centres, values, lam: float = 0.2) -> TPS:
     """FP64 GPU solve; centres = TPS kernel centres, values = mapped points."""
+    n = _pair_count(centres, values, "tps_solve")
     c = _markers(centres)
     v = _markers(values)
-    n = len(np.asarray(centres).reshape(-1, 3))
     h = C.c_void_p()
     _check(ctx.lib.tw_tps_solve(ctx.handle, c, v, n, lam, C.byref(h)), ctx, "tw_tps_solve")
     return TPS(ctx, h, n)
@@ -200,7 +211,7 @@ def warp_tps_device(ctx: Context, nodes, g: int, src, dst, interp: int = 0, stre
 def fit_affine(ctx: Context, tar, sub) -> np.ndarray:
     """4x4 matrix T with sub = T tar (3-D DLT, FP64 on the GPU)."""
     M = np.zeros(16, np.float64)
-    n = len(np.asarray(tar).reshape(-1, 3))
+    n = _pair_count(tar, sub, "fit_affine")
     _check(ctx.lib.tw_fit_affine(ctx.handle, _markers(tar), _markers(sub), n, M.ctypes.data_as(L._DP)), ctx,
            "tw_fit_affine")
     return M.reshape(4, 4)
@@ -213,7 +224,7 @@ def fit_affine_noalloc(ctx: Context, tar, sub) -> np.ndarray:
     """fit_affine through tw_fit_affine_noalloc: same result, no allocation;
     at most FIT_AFFINE_NOALLOC_MAX landmark pairs."""
     M = np.zeros(16, np.float64)
-    n = len(np.asarray(tar).reshape(-1, 3))
+    n = _pair_count(tar, sub, "fit_affine_noalloc")
     _check(ctx.lib.tw_fit_affine_noalloc(ctx.handle, _markers(tar), _markers(sub), n, M.ctypes.data_as(L._DP)),
            ctx, "tw_fit_affine_noalloc")
     return M.reshape(4, 4)
@@ -342,7 +353,7 @@ def imgwarp_smallmemory_tiled(ctx: Context, ql_marker_tar, ql_marker_sub, marker
     ql_marker_tar, both scaled by marker_scale."""
     if out is None and write_fn is None:
         out = _like(src, tuple(src.shape))
-    n = len(np.asarray(ql_marker_tar).reshape(-1, 3))
+    n = _pair_count(ql_marker_tar, ql_marker_sub, "imgwarp_smallmemory_tiled")
     rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
     opts = _tile_opts(tile, depth, interp)
     _check(ctx.lib.tw_imgwarp_smallmemory_tiled(ctx.handle, _markers(ql_marker_tar), _markers(ql_marker_sub), n,
@@ -405,10 +416,11 @@ class Server:
         s, d = _sz3(src), _sz3(dst)
         for a in range(3):
             j.src_sz[a], j.dst_sz[a] = s[a], d[a]
+        n = _pair_count(centres, values, "submit_tps")
         c, v = _markers(centres), _markers(values)
         j.centres = C.cast(c, C.POINTER(L.tw_marker))
         j.values = C.cast(v, C.POINTER(L.tw_marker))
-        j.n = len(np.asarray(centres).reshape(-1, 3))
+        j.n = n
         j.lambda_ = lam
         j.src, j.dst = _ptr(src), _ptr(dst)
         return self._submit(j, (src, dst, c, v))
@@ -471,7 +483,7 @@ def bigimagewarp(ctx: Context, p_img_sub, marker_sub=None, marker_tar=None, out=
     shape = (osz[2], osz[1], osz[0]) if len(p_img_sub.shape) == 3 else (sz4[3], osz[2], osz[1], osz[0])
     if out is None:
         out = _like(p_img_sub, shape)
-    n = 0 if marker_sub is None else len(np.asarray(marker_sub).reshape(-1, 3))
+    n = 0 if marker_sub is None else _pair_count(marker_sub, marker_tar, "bigimagewarp")
     ms = _markers(marker_sub if marker_sub is not None else np.zeros((1, 3)))
     mt = _markers(marker_tar if marker_tar is not None else np.zeros((1, 3)))
     _check(ctx.lib.tw_bigimagewarp(ctx.handle, C.byref(p), ms, mt, n, _dtype_code(p_img_sub),

@@ -4,7 +4,10 @@
 // The fit itself is the same kernel tw_fit_affine launches (3-D DLT with
 // Hartley normalisation, FP64), so the two return the same matrix.  What
 // differs is only where the landmark copies, the result and the status word
-// live: in g_fit_scratch below, whose address is looked up once per device.
+// live: in g_fit_scratch below, whose address is looked up once per device
+// context (again if that context was destroyed and created anew).
+
+#include <cuda.h>
 
 #include <mutex>
 
@@ -27,8 +30,16 @@ constexpr int kMaxDevices = 64;
 constexpr size_t kScratchDoubles = 9 * (size_t)kMaxN + 17;
 static __device__ __align__(256) double g_fit_scratch[kScratchDoubles];
 
+// g_fit_scratch's device address on each device, and the id of the device
+// context it was looked up in (0 = unknown).  A context that was destroyed
+// (cudaDeviceReset) and created again has a new id, so the lookup is redone
+// instead of handing the kernel an address from the old context.
+struct ScratchAddr {
+    double *ptr = nullptr;
+    unsigned long long ctx_id = 0;
+};
 std::mutex g_mu[kMaxDevices];              // one caller at a time per device
-double *g_addr[kMaxDevices] = {nullptr};   // g_fit_scratch on each device
+ScratchAddr g_addr[kMaxDevices];
 
 static_assert(sizeof(tw_marker) == 3 * sizeof(float), "tw_marker must be three packed floats");
 
@@ -41,6 +52,53 @@ __global__ void k_stage_markers(const float *t32, const float *s32, int m, doubl
         s[k] = s32[k];
     }
 }
+
+// Id of the calling thread's current device context through the driver API
+// (looked up through the runtime, so the library needs no -lcuda); 0 when the
+// driver offers no such query.
+unsigned long long current_ctx_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Puts the caller's current device back when the call returns.
+struct DeviceRestore {
+    int dev = -1;
+    DeviceRestore() { if (cudaGetDevice(&dev) != cudaSuccess) { dev = -1; cudaGetLastError(); } }
+    ~DeviceRestore() { if (dev >= 0) cudaSetDevice(dev); }
+};
+
+// Waits for the context's stream before the per-device lock is released, on
+// every return path: work already queued on the scratch array (copies, the
+// fit kernel) must finish before another call may touch it.
+struct StreamDrain {
+    cudaStream_t st;
+    ~StreamDrain()
+    {
+        if (st && cudaStreamSynchronize(st) != cudaSuccess) cudaGetLastError();
+    }
+};
 
 }  // namespace
 }  // namespace tw
@@ -57,14 +115,20 @@ tw_status tw_fit_affine_noalloc(tw_ctx *ctx, const tw_marker *tar, const tw_mark
                     "use tw_fit_affine for more");
     if (ctx->device < 0 || ctx->device >= kMaxDevices)
         return fail(ctx, TW_ERR_ARG, "tw_fit_affine_noalloc supports device indices 0..63");
+    DeviceRestore restore;
     std::lock_guard<std::mutex> lock(g_mu[ctx->device]);
     TW_CUDA_TRY(cudaSetDevice(ctx->device));
-    double *base = g_addr[ctx->device];
-    if (!base) {
-        // set-up, once per device, with that device current
-        TW_CUDA_TRY(cudaGetSymbolAddress((void **)&base, g_fit_scratch));
-        g_addr[ctx->device] = base;
+    StreamDrain drain{ctx->stream};  // declared after the lock: runs before it is released
+    ScratchAddr &sa = g_addr[ctx->device];
+    const unsigned long long id = current_ctx_id();
+    if (!sa.ptr || (id != 0 && id != sa.ctx_id)) {
+        // set-up, once per device context, with that device current
+        double *p = nullptr;
+        TW_CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_fit_scratch));
+        sa.ptr = p;
+        sa.ctx_id = id;
     }
+    double *base = sa.ptr;
     double *t64 = base;
     double *s64 = base + 3 * (size_t)kMaxN;
     float *t32 = reinterpret_cast<float *>(base + 6 * (size_t)kMaxN);

@@ -25,41 +25,55 @@ def _hash_noise(torch, n: int, seed: int, hi: int, device, start: int = 0) -> "t
 
 
 def blob_volume(shape_zyx, dtype: str, seed: int, n_blobs: int | None = None, sigma=(2.0, 8.0), peak=None,
-                noise: int = 10, n_fibres: int = 0, fibre_len: int = 400, fibre_value=None, device="cpu"):
+                noise: int = 10, n_fibres: int = 0, fibre_len: int = 400, fibre_value=None, device="cpu",
+                z_range=None):
     """Sum of seeded 3-D Gaussian blobs, clamped to the type's range, plus
     uniform integer noise and optional 1-voxel-wide random-walk fibres.
-    Returns a torch tensor (z, y, x) of dtype uint8 or uint16."""
+    Returns a torch tensor (z, y, x) of dtype uint8 or uint16.
+
+    The result is the same bytes on every device: the Gaussian factors are
+    computed on the host in numpy and only multiplied and summed (exactly
+    rounded float32 operations, in the same order) on the device.  With
+    z_range = (z0, z1) only planes z0..z1-1 of the volume of shape_zyx are
+    made (identical to those planes of the whole volume)."""
     import torch
     Z, Y, X = (int(v) for v in shape_zyx)
+    zr0, zr1 = (0, Z) if z_range is None else (int(z_range[0]), int(z_range[1]))
+    if not 0 <= zr0 < zr1 <= Z:
+        raise ValueError(f"z_range {z_range} outside the volume's {Z} planes")
     rng = np.random.default_rng(seed)
     vmax = 255 if dtype == "u8" else 4095
     if peak is None:
         peak = (40.0, 255.0) if dtype == "u8" else (400.0, 4095.0)
     if n_blobs is None:
         n_blobs = max(1, int(200 * (X * Y * Z) / (256 * 256 * 128)))
-    vol = torch.empty((Z, Y, X), dtype=torch.float32, device=device)
+    NZ = zr1 - zr0
+    vol = torch.empty((NZ, Y, X), dtype=torch.float32, device=device)
     step = max(1, (1 << 26) // (X * Y))  # noise in chunks of ~64 M voxels
-    for z0 in range(0, Z, step):
-        z1 = min(Z, z0 + step)
+    for z0 in range(zr0, zr1, step):
+        z1 = min(zr1, z0 + step)
         n0 = z0 * X * Y
-        vol[z0:z1] = _hash_noise(torch, (z1 - z0) * X * Y, seed, noise, device, n0).reshape(z1 - z0, Y, X)
+        vol[z0 - zr0:z1 - zr0] = _hash_noise(torch, (z1 - z0) * X * Y, seed, noise, device, n0).reshape(
+            z1 - z0, Y, X)
     cen = rng.uniform([0, 0, 0], [X, Y, Z], size=(n_blobs, 3))
     sig = rng.uniform(sigma[0], sigma[1], size=n_blobs)
     pk = rng.uniform(peak[0], peak[1], size=n_blobs)
+
+    def gauss(lo, hi, c, inv):
+        t = np.arange(lo, hi, dtype=np.float32) - np.float32(c)
+        return torch.as_tensor(np.exp((t * t).astype(np.float64) * inv).astype(np.float32), device=device)
+
     for (cx, cy, cz), s, p in zip(cen, sig, pk):
         r = int(math.ceil(3 * s))
         x0, x1 = max(0, int(cx) - r), min(X, int(cx) + r + 1)
         y0, y1 = max(0, int(cy) - r), min(Y, int(cy) + r + 1)
-        z0, z1 = max(0, int(cz) - r), min(Z, int(cz) + r + 1)
+        z0, z1 = max(zr0, int(cz) - r), min(zr1, int(cz) + r + 1)
         if x0 >= x1 or y0 >= y1 or z0 >= z1:
             continue
-        xs = torch.arange(x0, x1, device=device, dtype=torch.float32) - float(cx)
-        ys = torch.arange(y0, y1, device=device, dtype=torch.float32) - float(cy)
-        zs = torch.arange(z0, z1, device=device, dtype=torch.float32) - float(cz)
         inv = -0.5 / (s * s)
-        g = (torch.exp(zs * zs * inv)[:, None, None] * torch.exp(ys * ys * inv)[None, :, None]
-             * torch.exp(xs * xs * inv)[None, None, :])
-        vol[z0:z1, y0:y1, x0:x1] += float(p) * g
+        g = (gauss(z0, z1, cz, inv)[:, None, None] * gauss(y0, y1, cy, inv)[None, :, None]
+             * gauss(x0, x1, cx, inv)[None, None, :])
+        vol[z0 - zr0:z1 - zr0, y0:y1, x0:x1] += float(p) * g
     if n_fibres > 0:
         fv = fibre_value or ((200, 255) if dtype == "u8" else (2500, 4095))
         start = rng.uniform([0, 0, 0], [X, Y, Z], size=(n_fibres, 1, 3))
@@ -71,12 +85,14 @@ def blob_volume(shape_zyx, dtype: str, seed: int, n_blobs: int | None = None, si
         ok = (pts[:, 0] >= 0) & (pts[:, 0] < X) & (pts[:, 1] >= 0) & (pts[:, 1] < Y) & (pts[:, 2] >= 0) & (pts[:, 2] < Z)
         pts = pts[ok]
         vals = rng.uniform(fv[0], fv[1], size=len(pts)).astype(np.float32)
-        lin = torch.as_tensor(pts[:, 2] * Y * X + pts[:, 1] * X + pts[:, 0], device=device)
+        inz = (pts[:, 2] >= zr0) & (pts[:, 2] < zr1)
+        pts, vals = pts[inz], vals[inz]
+        lin = torch.as_tensor((pts[:, 2] - zr0) * Y * X + pts[:, 1] * X + pts[:, 0], device=device)
         flat = vol.view(-1)
         flat.index_put_((lin,), torch.as_tensor(vals, device=device))
-    out = torch.empty((Z, Y, X), dtype=torch.uint8 if dtype == "u8" else torch.uint16, device=device)
-    for z0 in range(0, Z, step):
-        z1 = min(Z, z0 + step)
+    out = torch.empty((NZ, Y, X), dtype=torch.uint8 if dtype == "u8" else torch.uint16, device=device)
+    for z0 in range(0, NZ, step):
+        z1 = min(NZ, z0 + step)
         out[z0:z1] = vol[z0:z1].clamp_(0, vmax).round_().to(torch.int32).to(out.dtype)
     return out
 
@@ -222,17 +238,18 @@ def plain_tps_case(seed: int = 1235, device="cpu", shape_zyx=(128, 256, 256), n:
 
 
 def large_tps_case(seed: int = 1237, device="cpu", shape_zyx=(1024, 2048, 2048), n: int = 2000, g: int = 16,
-                   n_blobs: int | None = None, n_fibres: int | None = None) -> Case:
+                   n_blobs: int | None = None, n_fibres: int | None = None, z_range=None) -> Case:
     """Large TPS: uint16 blob+fibre volume (values 0-4095), landmarks on a
     jittered lattice, targets displaced by 8 random-phase sinusoids
-    (amplitude <= 12) + N(0, 1)."""
+    (amplitude <= 12) + N(0, 1).  z_range = (z0, z1) makes only those planes
+    of the volume (the landmarks are those of the whole volume)."""
     Z, Y, X = shape_zyx
     vox = X * Y * Z
     if n_blobs is None:
         n_blobs = max(50, min(20000, int(200 * vox / (256 * 256 * 128))))
     if n_fibres is None:
         n_fibres = max(10, min(5000, vox // (1 << 20)))
-    vol = blob_volume(shape_zyx, "u16", seed, n_blobs=n_blobs, n_fibres=n_fibres, device=device)
+    vol = blob_volume(shape_zyx, "u16", seed, n_blobs=n_blobs, n_fibres=n_fibres, device=device, z_range=z_range)
     sub, tar = lattice_landmarks((X, Y, Z), n, seed + 7)
     return Case(f"large_tps_{X}x{Y}x{Z}_u16_n{n}_g{g}", vol, sub, tar, g)
 

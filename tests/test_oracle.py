@@ -152,3 +152,18 @@ def test_parallel_and_serial_oracle_agree():
     a = O.imgwarp_smallmemory_image(t, s, 4, src, threads=1)
     b = O.imgwarp_smallmemory_image(t, s, 4, src, threads=0)
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("box", [((13, 7, 5), (30, 20, 17)), ((0, 0, 0), (60, 50, 40)), ((59, 49, 39), (1, 1, 1))])
+def test_box_warp_equals_the_whole_warp_on_that_box(box):
+    rng = np.random.default_rng(0)
+    src = rng.integers(0, 4096, size=(40, 50, 60)).astype(np.uint16)
+    tar = rng.uniform(3, [57, 47, 37], size=(20, 3)).astype(np.float32)
+    sub = (tar + rng.normal(0, 3, size=tar.shape)).astype(np.float32)
+    c, d = O.tps_solve(tar, sub)
+    g = 8
+    df = O.tps_grid(tar, c, d, (O.grid_size(60, g), O.grid_size(50, g), O.grid_size(40, g)), g)
+    (ox, oy, oz), (nx, ny, nz) = box
+    full = O.tps_warp(src, df, g)
+    np.testing.assert_array_equal(O.tps_warp_box(src, df, g, (ox, oy, oz), (nx, ny, nz)),
+                                  full[oz:oz + nz, oy:oy + ny, ox:ox + nx])

@@ -51,12 +51,46 @@ def test_rejects_more_landmarks_than_its_limit(ctx):
 
 
 def test_allocates_no_device_memory(ctx):
+    """Free memory of the context's device is unchanged by the calls.  This
+    reads the device-wide figure, so it assumes that no other process
+    allocates on that GPU meanwhile (the test runs its calls back to back)."""
     tar, sub = landmark_set(7, 500)
     tw.fit_affine_noalloc(ctx, tar, sub)  # set-up on this device happens by now
-    torch.cuda.synchronize()
-    free0, _ = torch.cuda.mem_get_info(0)
+    torch.cuda.synchronize(ctx.device)
+    free0, _ = torch.cuda.mem_get_info(ctx.device)
     for s in range(5):
         tar, sub = landmark_set(30 + s, 100 + 700 * s)
         tw.fit_affine_noalloc(ctx, tar, sub)
-    free1, _ = torch.cuda.mem_get_info(0)
+    free1, _ = torch.cuda.mem_get_info(ctx.device)
     assert free1 == free0
+
+
+def test_concurrent_callers_on_two_contexts_get_their_own_results(ctx):
+    """Two contexts on one device share the scratch array; calls from two
+    threads (ctypes releases the GIL during the call) must be serialised by
+    the library so that each caller gets the matrix of its own landmarks."""
+    import threading
+
+    sets = [[landmark_set(100 + 10 * t + i, 64 + 97 * i) for i in range(12)] for t in range(2)]
+    want = [[tw.fit_affine(ctx, tar, sub) for tar, sub in s] for s in sets]
+    ctxs = [tw.Context(ctx.device), tw.Context(ctx.device)]
+    got = [[None] * 12 for _ in range(2)]
+    errors = []
+
+    def run(t):
+        try:
+            for rep in range(3):
+                for i, (tar, sub) in enumerate(sets[t]):
+                    got[t][i] = tw.fit_affine_noalloc(ctxs[t], tar, sub)
+                    np.testing.assert_allclose(got[t][i], want[t][i], rtol=0, atol=ATOL)
+        except Exception as e:  # reported on the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(t,)) for t in range(2)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    for c in ctxs:
+        c.close()
+    assert not errors, errors[0]
