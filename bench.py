@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--no-affine", action="store_true", help="skip the affine leg")
     ap.add_argument("--no-tiled", action="store_true", help="skip the tiled (out-of-core) leg")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error figures against the FP64 oracle")
-    ap.add_argument("--serve-jobs", type=int, default=32, help="jobs in the serving leg")
+    ap.add_argument("--serve-jobs", type=int, default=1000, help="jobs in the serving leg")
     ap.add_argument("--small", action="store_true", help="256x256x128 case, 64 landmarks")
     ap.add_argument("--shape", type=str, default="", help="X,Y,Z volume for profiling captures (default: full)")
     return ap.parse_args()
@@ -352,14 +352,44 @@ def tiled_leg(ctx, device: int, shape_zyx=(512, 2048, 2048)):
 
 # ------------------------------------------------------------- serving leg
 
+class _RingAlloc:
+    """Recycled output buffers: slices of one preallocated buffer handed out in
+    submission order; a slice is reused once the job that held it finished
+    (wait(job) is called for jobs whose slice would be overwritten)."""
+
+    def __init__(self, nbytes: int, wait):
+        self.n, self.head, self.live, self.wait = nbytes, 0, [], wait
+
+    def take(self, nbytes: int, job_key) -> int:
+        if nbytes > self.n:
+            raise ValueError("job larger than the output ring")
+        start = self.head if self.head + nbytes <= self.n else 0
+        end = start + nbytes
+        keep = []
+        for (k, a, b) in self.live:
+            if a < end and start < b:
+                self.wait(k)
+            else:
+                keep.append((k, a, b))
+        self.live = keep + [(job_key, start, end)]
+        self.head = end
+        return start
+
+
 def serving_leg(ctx, device: int, n_jobs: int, seed: int = 1239, rate_hz: float = 20.0):
     """The serving mix (Poisson arrivals at rate_hz, dims log-uniform 128^3 ..
     1024x1024x256, u8/u16, 30% affine / 10% rigid / 60% TPS with 16-4096
-    landmarks) through the continuous-batching server from pinned host
-    buffers: p50/p99 job latency (submit to result in host memory) and
-    aggregate GVoxel/s; the same jobs submitted all at once (capacity); and the
-    plain one-job-at-a-time path (operator-level call per job, H2D and D2H
-    included) for comparison."""
+    landmarks) through the continuous-batching server.
+
+    host: volumes in pinned host memory (outputs in a recycled pinned ring):
+      p50/p99 job latency (submit -> result in host memory) under Poisson
+      arrivals, aggregate GVoxel/s, capacity with every job submitted at once,
+      and the plain one-job-at-a-time path (one operator-level call per job,
+      H2D and D2H included) on the same jobs.
+    device: the same jobs with volumes already in HBM (outputs in a recycled
+      device ring): capacity of the server against the plain one-job-at-a-time
+      GPU path (solve, node grid and warp per job, each waited for).
+    Stage times (queue wait, solve, resample) come from tw_server_job_times."""
     import numpy as np
     import torch
 
@@ -371,19 +401,53 @@ def serving_leg(ctx, device: int, n_jobs: int, seed: int = 1239, rate_hz: float 
     tdt = {"u8": torch.uint8, "u16": torch.uint16}
     esz = {"u8": 1, "u16": 2}
     nbytes = [int(np.prod(j.shape_zyx)) * esz[j.dtype] for j in jobs]
-    # inputs: views of one pinned pool of random bytes (jobs only read them)
-    pool = torch.empty(max(nbytes), dtype=torch.uint8, pin_memory=True)
-    pool.copy_(torch.randint(0, 256, (max(nbytes),), dtype=torch.uint8, device=dev))
-    srcs = [pool[:b].view(tdt[j.dtype]).reshape(j.shape_zyx) for j, b in zip(jobs, nbytes)]
-    outs = [torch.empty(j.shape_zyx, dtype=tdt[j.dtype], pin_memory=True) for j in jobs]
     vox = sum(int(np.prod(j.shape_zyx)) for j in jobs)
+    big = max(nbytes)
+    # inputs: views of one pool of random bytes (jobs only read them)
+    h_pool = torch.empty(big, dtype=torch.uint8, pin_memory=True)
+    h_pool.copy_(torch.randint(0, 256, (big,), dtype=torch.uint8, device=dev))
+    d_pool = h_pool.to(dev)
+    ring_bytes = max(4 * big, 4 << 30)
+    h_ring = torch.empty(ring_bytes, dtype=torch.uint8, pin_memory=True)
+    d_ring = torch.empty(ring_bytes, dtype=torch.uint8, device=dev)
+
+    def view(pool, off, j, b):
+        return pool[off:off + b].view(tdt[j.dtype]).reshape(j.shape_zyx)
 
     def submit(srv, j, src, dst):
         if j.kind == "tps":
             return srv.submit_tps(j.centres, j.values, j.g, src, dst)
         return srv.submit_affine(j.M, src, dst)
 
-    def plain(j, src, dst):
+    def served(srv, pool, ring_pool, poisson: bool):
+        ids = {}
+        ring = _RingAlloc(ring_bytes, lambda k: srv.wait(ids[k]))
+        t0 = time.perf_counter()
+        for i, (j, b) in enumerate(zip(jobs, nbytes)):
+            if poisson:
+                delay = t0 + j.arrival_s - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+            off = ring.take(b, i)
+            ids[i] = submit(srv, j, view(pool, 0, j, b), view(ring_pool, off, j, b))
+        lats = [srv.wait(ids[i]) for i in range(len(jobs))]
+        wall = time.perf_counter() - t0
+        times = [srv.job_times(ids[i]) for i in range(len(jobs))]
+        return wall, lats, times
+
+    def pct(v, q):
+        v = [x for x in v if x is not None]
+        return float(np.percentile(v, q)) * 1e3 if v else None
+
+    def stage_summary(times):
+        solve = [t["solve"] for t in times]
+        rs = [None if t["resample_start"] is None else t["resample_end"] - t["resample_start"] for t in times]
+        queued = [t["queued"] for t in times]
+        return {"queued_p50_ms": pct(queued, 50), "queued_p99_ms": pct(queued, 99),
+                "solve_done_p50_ms": pct(solve, 50), "resample_round_p50_ms": pct(rs, 50),
+                "resample_round_p99_ms": pct(rs, 99)}
+
+    def plain_host(j, src, dst):
         if j.kind == "tps":
             tw.imgwarp_smallmemory_image(ctx, j.values, j.centres, j.g, j.g, j.g, 1, 0, src, out=dst)
         else:
@@ -393,45 +457,56 @@ def serving_leg(ctx, device: int, n_jobs: int, seed: int = 1239, rate_hz: float 
             dst.copy_(d_dst)
         torch.cuda.synchronize()
 
-    warm = list(range(min(4, n_jobs)))
+    def plain_device(j, src, dst):
+        if j.kind == "tps":
+            Z, Y, X = j.shape_zyx
+            t = tw.tps_solve(ctx, j.centres, j.values)
+            nodes = tw.tps_eval_grid(ctx, t, (tw.grid_size(X, j.g), tw.grid_size(Y, j.g), tw.grid_size(Z, j.g)), j.g)
+            tw.warp_tps_device(ctx, nodes, j.g, src, dst)
+            t.close()
+        else:
+            tw.warp_affine_device(ctx, j.M, src, dst)
+        torch.cuda.synchronize()
+
+    def sequential(plain, pool, ring_pool):
+        for i in range(min(4, len(jobs))):  # warm
+            plain(jobs[i], view(pool, 0, jobs[i], nbytes[i]), view(ring_pool, 0, jobs[i], nbytes[i]))
+        t0 = time.perf_counter()
+        off = 0
+        for j, b in zip(jobs, nbytes):
+            off = 0 if off + b > ring_bytes else off
+            plain(j, view(pool, 0, j, b), view(ring_pool, off, j, b))
+            off += b
+        return time.perf_counter() - t0
+
+    out = {"jobs": n_jobs, "rate_hz": rate_hz,
+           "mix": {k: sum(1 for j in jobs if j.kind == k) for k in ("affine", "rigid", "tps")}, "voxels": vox}
     with api.Server(ctx) as srv:
-        # untimed pass over every job at once: grows the server's memory pool
-        # to the working set and loads every kernel variant the mix uses
-        for i in [submit(srv, j, src, dst) for j, src, dst in zip(jobs, srcs, outs)]:
-            srv.wait(i)
-        # Poisson arrivals
-        t0 = time.perf_counter()
-        ids = []
-        for j, src, dst in zip(jobs, srcs, outs):
-            delay = t0 + j.arrival_s - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            ids.append(submit(srv, j, src, dst))
-        lats = [srv.wait(i) for i in ids]
-        t_poisson = time.perf_counter() - t0
-        # capacity: every job submitted at once
-        t0 = time.perf_counter()
-        ids = [submit(srv, j, src, dst) for j, src, dst in zip(jobs, srcs, outs)]
-        for i in ids:
-            srv.wait(i)
-        t_sat = time.perf_counter() - t0
-    for i in warm:
-        plain(jobs[i], srcs[i], outs[i])
-    t0 = time.perf_counter()
-    for j, src, dst in zip(jobs, srcs, outs):
-        plain(j, src, dst)
-    t_seq = time.perf_counter() - t0
+        served(srv, h_pool, h_ring, False)  # untimed: grows the pools, loads every kernel variant
+        wall_p, lats, times_p = served(srv, h_pool, h_ring, True)
+        wall_s, _, times_s = served(srv, h_pool, h_ring, False)
+    t_seq = sequential(plain_host, h_pool, h_ring)
     lat_ms = sorted(1e3 * v for v in lats)
-    kinds = {k: sum(1 for j in jobs if j.kind == k) for k in ("affine", "rigid", "tps")}
-    return {
-        "jobs": n_jobs, "rate_hz": rate_hz, "mix": kinds, "voxels": vox,
+    out["host"] = {
         "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
-        "poisson_gvoxel_s": vox / t_poisson / 1e9, "poisson_wall_s": t_poisson,
-        "saturated_gvoxel_s": vox / t_sat / 1e9,
-        "sequential_gvoxel_s": vox / t_seq / 1e9,
-        "saturated_over_sequential": t_seq / t_sat,
-        "path": "tw_server_* from pinned host buffers vs one operator-level call per job",
-    }
+        "poisson_gvoxel_s": vox / wall_p / 1e9, "poisson_wall_s": wall_p,
+        "saturated_gvoxel_s": vox / wall_s / 1e9, "sequential_gvoxel_s": vox / t_seq / 1e9,
+        "saturated_over_sequential": t_seq / wall_s,
+        "stages_poisson": stage_summary(times_p), "stages_saturated": stage_summary(times_s),
+        "path": "tw_server_* from pinned host buffers (recycled output ring) vs one operator-level call per job"}
+    with api.Server(ctx) as srv:
+        served(srv, d_pool, d_ring, False)
+        wall_d, lats_d, times_d = served(srv, d_pool, d_ring, False)
+    t_seq_d = sequential(plain_device, d_pool, d_ring)
+    lat_d = sorted(1e3 * v for v in lats_d)
+    out["device"] = {
+        "saturated_gvoxel_s": vox / wall_d / 1e9, "sequential_gvoxel_s": vox / t_seq_d / 1e9,
+        "saturated_over_sequential": t_seq_d / wall_d,
+        "saturated_p50_ms": float(np.percentile(lat_d, 50)), "saturated_p99_ms": float(np.percentile(lat_d, 99)),
+        "stages": stage_summary(times_d),
+        "path": "tw_server_* on device-resident volumes vs solve + node grid + warp per job, each waited for"}
+    del h_pool, d_pool, h_ring, d_ring
+    return out
 
 
 # ----------------------------------------------------------- accuracy

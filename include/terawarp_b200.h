@@ -278,6 +278,10 @@ typedef struct {
     double marker_scale;    /* 0 = 1.0 (whole image); the reference's tiled path uses 4 */
     double lambda;          /* 0 = 0.2 (q_imgwarp_tps_quicksmallmemory.cpp:581)       */
     int interp;             /* tw_interp                                              */
+    int downsample_mode;    /* 1: also write a downsampled preview of the result
+                               (the plugin's downsample_mode,
+                               plugin_Bigimagewarp.cpp:93, :264-325; used by
+                               tw_bigimagewarp_files)                                 */
 } tw_params;
 
 /* Fills *p with the reference's defaults (TPS, GPU, spacing 4, lambda 0.2). */
@@ -302,6 +306,77 @@ int tw_downsample_factor(const int64_t sz[3]);
 tw_status tw_downsample_image(tw_ctx *ctx, int dtype, const void *img, const int64_t sz[4],
                               void *img_out, int64_t out_sz[3]);
 
+/* ------------------------------------------------------------------- files */
+
+/* Vaa3D raw stacks (.v3draw, and the .raw slice files of the tiled path), as
+ * the reference reads them in loadMetadata_cyf (RawFmtMngr.cpp:332-446) and
+ * writes them in saveStack2Raw_cyf (Bigwarp.cpp:660-751): the 24-byte key
+ * "raw_image_stack_by_hpeng", one endianness byte ('L' or 'B'), a 2-byte data
+ * type code (bytes per voxel: 1, 2 or 4), four 4-byte sizes x, y, z,
+ * channels, then the voxels, x fastest.  Files of either byte order are
+ * read; files are written in the host's order.  dtype is TW_U8, TW_U16, or 4
+ * for a float32 stack (readable, not warpable).  These functions use no GPU. */
+tw_status tw_v3draw_read_header(const char *path, int64_t sz[4], int *dtype, int64_t *header_bytes);
+/* Reads the whole payload (every channel) into dst (dst_bytes at least
+ * x*y*z*channels*bytes per voxel). */
+tw_status tw_v3draw_read(const char *path, void *dst, size_t dst_bytes);
+/* Reads box [x0,x0+nx) x [y0,y0+ny) x [z0,z0+nz) of channel 0 into dst (x
+ * fastest, pitch nx, nx*ny); replaces copyRawFileBlock2Buffer_cyf
+ * (RawFmtMngr.cpp:1511-1695), with one positioned read per row run. */
+tw_status tw_v3draw_read_box(const char *path, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny,
+                             int64_t nz, void *dst);
+tw_status tw_v3draw_write(const char *path, const void *data, const int64_t sz[4], int dtype);
+
+/* A directory of per-Z raw slice files (one x*y plane each) as a tile source:
+ * the files are every entry but ".", "..", "mdata.bin" and ".iim.format",
+ * sorted by name, one per z (read_2Dtif_dir, dir_make.cpp:175-216); all must
+ * share plane size and type.  threads: planes read in parallel (0 = up to
+ * 16).  Replaces read_2Dtif_BLOCK (Bigwarp.cpp:66-175). */
+typedef struct tw_slice_dir tw_slice_dir;
+tw_status tw_slice_dir_open(const char *dir, int threads, tw_slice_dir **out);
+tw_status tw_slice_dir_info(const tw_slice_dir *d, int64_t sz[3], int *dtype);
+tw_status tw_slice_dir_close(tw_slice_dir *d);
+/* tw_read_box_fn over a tw_slice_dir (user = tw_slice_dir*). */
+int tw_box_reader_slices(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                         void *dst);
+
+/* A tile sink that writes finished output tiles straight into per-Z raw
+ * slice files in `dir` (created if needed), named as the reference names its
+ * stitched output: "%07d.raw" of z * 10 (saveImage_PJ, Bigwarp.cpp:957-1004).
+ * Every slice file is created at its full size by tw_slice_writer_create, so
+ * tiles may arrive in any order; this replaces saving tiles and stitching
+ * them into slices in a second pass (Bigwarp.cpp:229-573, :958-1121). */
+typedef struct tw_slice_writer tw_slice_writer;
+tw_status tw_slice_writer_create(const char *dir, const int64_t sz[3], int dtype, int threads,
+                                 tw_slice_writer **out);
+tw_status tw_slice_writer_close(tw_slice_writer *w);
+/* tw_write_box_fn over a tw_slice_writer (user = tw_slice_writer*). */
+int tw_box_writer_slices(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                         const void *src);
+
+/* Vaa3D .marker files (read by readMarker_file, plugin_Bigimagewarp.cpp:145):
+ * comma-separated lines "x,y,z,radius,shape,name,comment,r,g,b"; lines that
+ * start with '#' and lines without three leading numbers are skipped.  x, y, z
+ * are returned as written (the plugin passes them to the warp unchanged).
+ * With out = NULL only *n is set; otherwise capacity must hold *n markers. */
+tw_status tw_marker_file_read(const char *path, tw_marker *out, int capacity, int *n);
+tw_status tw_marker_file_write(const char *path, const tw_marker *m, int n);
+
+/* The plugin's whole command on files (bigimagewarp,
+ * plugin_Bigimagewarp.cpp:123-336): reads the two marker files, then
+ *   - img_sub a .v3draw file: warps it in memory (tw_bigimagewarp) and writes
+ *     out_dir/<name><suffix>.v3draw;
+ *   - img_sub a directory of slices: warps it tile by tile from the slices
+ *     into out_dir/<name><suffix>_slice/ (slice files, written as tiles finish);
+ * with suffix _affine, _stps, _scaling, _rotation or _translation by mode.
+ * downsample_mode 1 also writes the downsampled preview (factor
+ * tw_downsample_factor) as <name><suffix>_downsample.v3draw or
+ * <name><suffix>_downsample_slice/.  marker_scale 0 means the reference's
+ * choice: 1 for a .v3draw, 4 for a slice directory
+ * (q_imgwarp_tps_quicksmallmemory.cpp:1194-1203, q_warp_affine_tps.cpp:866-874). */
+tw_status tw_bigimagewarp_files(tw_ctx *ctx, const tw_params *p, const char *img_sub, const char *marker_sub,
+                                const char *marker_tar, const char *out_dir);
+
 /* ------------------------------------------------------------- serving loop */
 
 typedef struct tw_server tw_server;
@@ -317,8 +392,10 @@ typedef struct {
     const tw_marker *centres, *values; /* TPS landmarks (kind 1), copied at submit   */
     int n;
     double lambda;          /* 0 = 0.2                                               */
-    const void *src;        /* host input (pinned or pageable), read after submit    */
-    void *dst;              /* host output, written before the job reports done      */
+    const void *src;        /* input: host (pinned or pageable) memory, copied to HBM
+                               after submit, or device memory, read in place         */
+    void *dst;              /* output: host memory (copied back) or device memory
+                               (written in place), complete when the job reports done */
 } tw_job;
 
 /* Continuous-batching server: a worker thread admits submitted jobs as soon
@@ -331,6 +408,16 @@ tw_status tw_server_submit(tw_server *s, const tw_job *job, uint64_t *job_id);
  * TW_ERR_NOT_READY while running, or the job's error. */
 tw_status tw_server_poll(tw_server *s, uint64_t job_id, double *latency_s);
 tw_status tw_server_wait(tw_server *s, uint64_t job_id, double timeout_s, double *latency_s);
+/* Stage times of a finished job, in seconds (-1 where a stage does not apply):
+ *   times[0] submit -> admission (host clock: queued behind the HBM budget
+ *            or the in-flight bound)
+ *   times[1..6] from admission, on the GPU clock (CUDA events): solve done,
+ *            node grid done, inputs resident, resample round started,
+ *            resample round ended, result in place (copied back, or written
+ *            in place for a device-resident job)
+ *   times[7] submit -> done (host clock, the latency tw_server_poll reports)
+ * TW_ERR_NOT_READY while the job runs.  No counterpart in the reference. */
+tw_status tw_server_job_times(tw_server *s, uint64_t job_id, double times[8]);
 tw_status tw_server_destroy(tw_server *s);
 
 #ifdef __cplusplus

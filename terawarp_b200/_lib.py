@@ -34,6 +34,7 @@ class tw_params(C.Structure):
         ("para_x", C.c_double), ("para_y", C.c_double), ("para_z", C.c_double),
         ("newsize_x", C.c_int64), ("newsize_y", C.c_int64), ("newsize_z", C.c_int64),
         ("grid_spacing", C.c_int), ("marker_scale", C.c_double), ("lambda_", C.c_double), ("interp", C.c_int),
+        ("downsample_mode", C.c_int),
     ]
 
 
@@ -91,10 +92,26 @@ SIGNATURES = {
     "tw_bigimagewarp": (C.c_int, [_P, C.POINTER(tw_params), _MP, _MP, C.c_int, C.c_int, _P, _I64P, _P]),
     "tw_downsample_factor": (C.c_int, [_I64P]),
     "tw_downsample_image": (C.c_int, [_P, C.c_int, _P, _I64P, _P, _I64P]),
+    "tw_v3draw_read_header": (C.c_int, [C.c_char_p, _I64P, C.POINTER(C.c_int), _I64P]),
+    "tw_v3draw_read": (C.c_int, [C.c_char_p, _P, C.c_size_t]),
+    "tw_v3draw_read_box": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                     _P]),
+    "tw_v3draw_write": (C.c_int, [C.c_char_p, _P, _I64P, C.c_int]),
+    "tw_slice_dir_open": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_P)]),
+    "tw_slice_dir_info": (C.c_int, [_P, _I64P, C.POINTER(C.c_int)]),
+    "tw_slice_dir_close": (C.c_int, [_P]),
+    "tw_box_reader_slices": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
+    "tw_slice_writer_create": (C.c_int, [C.c_char_p, _I64P, C.c_int, C.c_int, C.POINTER(_P)]),
+    "tw_slice_writer_close": (C.c_int, [_P]),
+    "tw_box_writer_slices": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
+    "tw_marker_file_read": (C.c_int, [C.c_char_p, _MP, C.c_int, C.POINTER(C.c_int)]),
+    "tw_marker_file_write": (C.c_int, [C.c_char_p, _MP, C.c_int]),
+    "tw_bigimagewarp_files": (C.c_int, [_P, C.POINTER(tw_params), C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]),
     "tw_server_create": (C.c_int, [_P, C.c_size_t, C.c_int, C.POINTER(_P)]),
     "tw_server_submit": (C.c_int, [_P, C.POINTER(tw_job), C.POINTER(C.c_uint64)]),
     "tw_server_poll": (C.c_int, [_P, C.c_uint64, _DP]),
     "tw_server_wait": (C.c_int, [_P, C.c_uint64, C.c_double, _DP]),
+    "tw_server_job_times": (C.c_int, [_P, C.c_uint64, _DP]),
     "tw_server_destroy": (C.c_int, [_P]),
 }
 

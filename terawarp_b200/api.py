@@ -303,18 +303,21 @@ def _host_volume(x) -> L.tw_host_volume:
 
 def _box_io(src, dst, read_fn=None, write_fn=None):
     """Tile source / sink: the library's built-in host-volume reader and writer
-    (strided DMA when the array is pinned), or Python callables
-    read_fn(x0, y0, z0, nx, ny, nz) -> array(nz, ny, nx) and
+    (strided DMA when the array is pinned), a SliceDir / SliceWriter, or
+    Python callables read_fn(x0, y0, z0, nx, ny, nz) -> array(nz, ny, nx) and
     write_fn(x0, y0, z0, block) for testing the callback path."""
     lib = L.load()
     keep = []
-    if read_fn is None:
+    if isinstance(src, SliceDir):
+        rd = L.READ_BOX(C.cast(lib.tw_box_reader_slices, C.c_void_p).value)
+        ru = src.handle
+    elif read_fn is None:
         hv_in = _host_volume(src)
         keep.append(hv_in)
         rd = L.READ_BOX(C.cast(lib.tw_box_reader_host, C.c_void_p).value)
         ru = C.cast(C.pointer(hv_in), C.c_void_p)
     else:
-        es = 1 if _dtype_code(src) == L.TW_U8 else 2
+        es = 1 if _src_dtype(src) == L.TW_U8 else 2
 
         def _rd(user, x0, y0, z0, nx, ny, nz, dstp):
             try:
@@ -325,13 +328,16 @@ def _box_io(src, dst, read_fn=None, write_fn=None):
                 return 1
         rd = L.READ_BOX(_rd)
         ru = None
-    if write_fn is None:
+    if isinstance(dst, SliceWriter):
+        wr = L.WRITE_BOX(C.cast(lib.tw_box_writer_slices, C.c_void_p).value)
+        wu = dst.handle
+    elif write_fn is None:
         hv_out = _host_volume(dst)
         keep.append(hv_out)
         wr = L.WRITE_BOX(C.cast(lib.tw_box_writer_host, C.c_void_p).value)
         wu = C.cast(C.pointer(hv_out), C.c_void_p)
     else:
-        dt = np.uint8 if _dtype_code(src) == L.TW_U8 else np.uint16
+        dt = np.uint8 if _src_dtype(src) == L.TW_U8 else np.uint16
 
         def _wr(user, x0, y0, z0, nx, ny, nz, srcp):
             try:
@@ -346,18 +352,29 @@ def _box_io(src, dst, read_fn=None, write_fn=None):
     return rd, ru, wr, wu, keep
 
 
+def _src_dtype(src) -> int:
+    return src.dtype_code if isinstance(src, SliceDir) else _dtype_code(src)
+
+
+def _src_sz3(src):
+    if isinstance(src, SliceDir):
+        return (C.c_int64 * 3)(*src.shape_xyz)
+    return _sz3(src)
+
+
 def imgwarp_smallmemory_tiled(ctx: Context, ql_marker_tar, ql_marker_sub, marker_scale: float, g: int, src, out=None,
                               tile=(512, 512, 512), depth: int = 2, interp: int = 0, read_fn=None, write_fn=None):
     """Mirror of imgwarp_smallmemory_CYF for volumes streamed tile by tile
     (the source may exceed HBM): centres = ql_marker_sub, values =
-    ql_marker_tar, both scaled by marker_scale."""
+    ql_marker_tar, both scaled by marker_scale.  src: a host array, or a
+    SliceDir; out: a host array, or a SliceWriter."""
     if out is None and write_fn is None:
         out = _like(src, tuple(src.shape))
     n = _pair_count(ql_marker_tar, ql_marker_sub, "imgwarp_smallmemory_tiled")
     rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
     opts = _tile_opts(tile, depth, interp)
     _check(ctx.lib.tw_imgwarp_smallmemory_tiled(ctx.handle, _markers(ql_marker_tar), _markers(ql_marker_sub), n,
-                                                marker_scale, g, _dtype_code(src), _sz3(src), rd, ru, wr, wu,
+                                                marker_scale, g, _src_dtype(src), _src_sz3(src), rd, ru, wr, wu,
                                                 C.byref(opts)), ctx, "tw_imgwarp_smallmemory_tiled")
     del keep
     return out
@@ -373,10 +390,156 @@ def warp_affine_tiled(ctx: Context, M, src, out_shape_zyx=None, out=None, tile=(
     rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
     opts = _tile_opts(tile, depth, interp)
     osz = (C.c_int64 * 3)(shape[2], shape[1], shape[0])
-    _check(ctx.lib.tw_warp_affine_tiled(ctx.handle, Mx.ctypes.data_as(L._DP), _dtype_code(src), _sz3(src), osz, rd,
+    _check(ctx.lib.tw_warp_affine_tiled(ctx.handle, Mx.ctypes.data_as(L._DP), _src_dtype(src), _src_sz3(src), osz, rd,
                                         ru, wr, wu, C.byref(opts)), ctx, "tw_warp_affine_tiled")
     del keep
     return out
+
+
+# ------------------------------------------------------------------- files
+
+def _io_check(status: int, what: str) -> None:
+    if status != L.TW_OK:
+        lib = L.load()
+        raise TeraWarpError(status, f"{what}: {(lib.tw_status_string(status) or b'').decode()}")
+
+
+def v3draw_header(path: str):
+    """((x, y, z, channels), dtype code) of a Vaa3D raw stack."""
+    sz = (C.c_int64 * 4)()
+    dt = C.c_int()
+    _io_check(L.load().tw_v3draw_read_header(str(path).encode(), sz, C.byref(dt), None), f"read header {path}")
+    return tuple(int(v) for v in sz), int(dt.value)
+
+
+def v3draw_read(path: str) -> np.ndarray:
+    """A raw stack as (z, y, x) (one channel) or (c, z, y, x)."""
+    (x, y, z, c), dt = v3draw_header(path)
+    npdt = {L.TW_U8: np.uint8, L.TW_U16: np.uint16, 4: np.float32}[dt]
+    a = np.empty((c, z, y, x), npdt)
+    _io_check(L.load().tw_v3draw_read(str(path).encode(), a.ctypes.data, a.nbytes), f"read {path}")
+    return a[0] if c == 1 else a
+
+
+def v3draw_read_box(path: str, o_xyz, n_xyz) -> np.ndarray:
+    """Box [o, o + n) of channel 0 as (nz, ny, nx)."""
+    (_, _, _, _), dt = v3draw_header(path)
+    npdt = {L.TW_U8: np.uint8, L.TW_U16: np.uint16, 4: np.float32}[dt]
+    nx, ny, nz = (int(v) for v in n_xyz)
+    a = np.empty((nz, ny, nx), npdt)
+    _io_check(L.load().tw_v3draw_read_box(str(path).encode(), int(o_xyz[0]), int(o_xyz[1]), int(o_xyz[2]), nx, ny,
+                                          nz, a.ctypes.data), f"read box of {path}")
+    return a
+
+
+def v3draw_write(path: str, arr) -> None:
+    a = np.ascontiguousarray(arr)
+    _io_check(L.load().tw_v3draw_write(str(path).encode(), a.ctypes.data, _sz4(a), _dtype_code(a)), f"write {path}")
+
+
+class SliceDir:
+    """A directory of per-Z raw slice files as a tile source (tw_slice_dir)."""
+
+    def __init__(self, path: str, threads: int = 0):
+        self.lib = L.load()
+        h = C.c_void_p()
+        _io_check(self.lib.tw_slice_dir_open(str(path).encode(), threads, C.byref(h)), f"open slices {path}")
+        self.handle = h
+        sz = (C.c_int64 * 3)()
+        dt = C.c_int()
+        self.lib.tw_slice_dir_info(h, sz, C.byref(dt))
+        self.shape_xyz = tuple(int(v) for v in sz)
+        self.shape = (self.shape_xyz[2], self.shape_xyz[1], self.shape_xyz[0])
+        self.dtype_code = int(dt.value)
+        self.dtype = np.uint8 if self.dtype_code == L.TW_U8 else np.uint16
+
+    def read_box(self, o_xyz, n_xyz) -> np.ndarray:
+        nx, ny, nz = (int(v) for v in n_xyz)
+        a = np.empty((nz, ny, nx), self.dtype)
+        rc = self.lib.tw_box_reader_slices(self.handle, int(o_xyz[0]), int(o_xyz[1]), int(o_xyz[2]), nx, ny, nz,
+                                           a.ctypes.data)
+        if rc != 0:
+            raise TeraWarpError(L.TW_ERR_IO, f"slice read failed ({rc})")
+        return a
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.tw_slice_dir_close(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class SliceWriter:
+    """Per-Z raw slice files that output tiles are written into (tw_slice_writer)."""
+
+    def __init__(self, path: str, shape_zyx, dtype, threads: int = 0):
+        self.lib = L.load()
+        self.dtype_code = L.TW_U8 if np.dtype(dtype) == np.uint8 else L.TW_U16
+        sz = (C.c_int64 * 3)(int(shape_zyx[2]), int(shape_zyx[1]), int(shape_zyx[0]))
+        h = C.c_void_p()
+        _io_check(self.lib.tw_slice_writer_create(str(path).encode(), sz, self.dtype_code, threads, C.byref(h)),
+                  f"create slices in {path}")
+        self.handle = h
+        self.shape = tuple(int(v) for v in shape_zyx)
+
+    def write_box(self, o_xyz, block) -> None:
+        b = np.ascontiguousarray(block)
+        nz, ny, nx = b.shape
+        rc = self.lib.tw_box_writer_slices(self.handle, int(o_xyz[0]), int(o_xyz[1]), int(o_xyz[2]), nx, ny, nz,
+                                           b.ctypes.data)
+        if rc != 0:
+            raise TeraWarpError(L.TW_ERR_IO, f"slice write failed ({rc})")
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.tw_slice_writer_close(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def read_slices(path: str) -> np.ndarray:
+    """A whole slice directory as one (z, y, x) array."""
+    with SliceDir(path) as d:
+        x, y, z = d.shape_xyz
+        return d.read_box((0, 0, 0), (x, y, z))
+
+
+def read_markers(path: str) -> np.ndarray:
+    """(n, 3) float32 x, y, z of a .marker file."""
+    lib = L.load()
+    n = C.c_int()
+    _io_check(lib.tw_marker_file_read(str(path).encode(), None, 0, C.byref(n)), f"read markers {path}")
+    buf = (L.tw_marker * max(1, n.value))()
+    _io_check(lib.tw_marker_file_read(str(path).encode(), buf, n.value, C.byref(n)), f"read markers {path}")
+    return np.frombuffer(bytes(buf), np.float32).reshape(-1, 3)[:n.value].copy()
+
+
+def write_markers(path: str, pts) -> None:
+    _io_check(L.load().tw_marker_file_write(str(path).encode(), _markers(pts), len(np.asarray(pts).reshape(-1, 3))),
+              f"write markers {path}")
+
+
+def bigimagewarp_files(ctx: Context, img_sub: str, marker_sub: str, marker_tar: str, out_dir: str,
+                       downsample_mode: int = 0, **kw) -> None:
+    """The plugin's command on files (tw_bigimagewarp_files): a .v3draw file or
+    a directory of slices in, <name><suffix>.v3draw or <name><suffix>_slice/
+    out (keyword arguments as `params`)."""
+    p = params(**kw)
+    p.downsample_mode = int(downsample_mode)
+    _check(ctx.lib.tw_bigimagewarp_files(ctx.handle, C.byref(p), str(img_sub).encode(),
+                                         str(marker_sub).encode() if marker_sub else None,
+                                         str(marker_tar).encode() if marker_tar else None, str(out_dir).encode()),
+           ctx, "tw_bigimagewarp_files")
 
 
 class Server:
@@ -441,6 +604,17 @@ class Server:
         self._keep.pop(job_id, None)
         _check(st, None, f"server job {job_id}")
         return lat.value
+
+    def job_times(self, job_id: int) -> dict:
+        """Stage times (seconds) of a finished job: queue wait before
+        admission, then solve / node grid / inputs resident / resample start /
+        resample end / result in place measured from admission on the GPU
+        clock (None where a stage does not apply), and the total latency."""
+        t = np.zeros(8, np.float64)
+        _check(self.ctx.lib.tw_server_job_times(self.handle, job_id, t.ctypes.data_as(L._DP)), None,
+               f"server job {job_id} times")
+        names = ["queued", "solve", "grid", "ready", "resample_start", "resample_end", "done", "latency"]
+        return {k: (None if v < 0 else float(v)) for k, v in zip(names, t)}
 
     def close(self) -> None:
         if self.handle:

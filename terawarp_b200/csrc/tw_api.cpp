@@ -101,6 +101,18 @@ tw_status upload(tw_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStre
     return TW_OK;
 }
 
+tw_status check_kernel_errors(tw_ctx *ctx)
+{
+    if (!ctx->d_err) return TW_OK;
+    int h = 0;
+    TW_CUDA_TRY(cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h == 0) return TW_OK;
+    TW_CUDA_TRY(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return fail(ctx, TW_ERR_TIMEOUT, "a resample kernel gave up waiting for a staged source plane");
+}
+
 int64_t grid_size(int64_t sz, int g) { return (int64_t)std::ceil((double)sz / (double)g) + 3; }
 
 bool is_device_ptr(const void *p)
@@ -128,7 +140,7 @@ static constexpr size_t kTpsAuxBytes = sizeof(double) * 16 + 16;
 
 // Device-resident TPS field of one job: coefficients + node grid.
 tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *values, int n, double lambda,
-                   double scale, cudaStream_t st, tw_tps **out, bool wait)
+                   double scale, cudaStream_t st, tw_tps **out, bool wait, double *h_stage)
 {
     *out = nullptr;
     if (!centres || !values || n < 4) return fail(ctx, TW_ERR_ARG, "TPS needs n >= 4 landmark pairs");
@@ -159,7 +171,7 @@ tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *value
     if (s == TW_OK) {
         t->d_status = reinterpret_cast<int *>(t->d_d + 16);
         s = solve_tps_device(ctx, hc.data(), hv.data(), n, lambda, t->d_c, t->d_d, t->d_status,
-                             wait ? t->h_d : nullptr, o, t->d_ctr32, t->d_coef32, st);
+                             wait ? t->h_d : nullptr, o, t->d_ctr32, t->d_coef32, st, h_stage);
     }
     if (s != TW_OK) {
         dfree_on(ctx, t->d_c, cbytes, st);
@@ -281,6 +293,8 @@ tw_status tw_ctx_create(int device, size_t hbm_budget_bytes, tw_ctx **out)
             return destroy_partial(c.release());
     if (cudaMallocHost((void **)&c->stage_h, tw_ctx::kStageBytes * tw_ctx::kStageSlots) != cudaSuccess)
         return destroy_partial(c.release());
+    if (cudaMalloc((void **)&c->d_err, 256) != cudaSuccess || cudaMemset(c->d_err, 0, 256) != cudaSuccess)
+        return destroy_partial(c.release());
     for (int s = 0; s < tw_ctx::kStageSlots; ++s)
         if (cudaEventCreateWithFlags(&c->stage_ev[s], cudaEventDisableTiming) != cudaSuccess)
             return destroy_partial(c.release());
@@ -306,6 +320,7 @@ tw_status tw_ctx_destroy(tw_ctx *ctx)
     for (int s = 0; s < tw_ctx::kStageSlots; ++s)
         if (ctx->stage_ev[s]) cudaEventDestroy(ctx->stage_ev[s]);
     if (ctx->stage_h) cudaFreeHost(ctx->stage_h);
+    if (ctx->d_err) cudaFree(ctx->d_err);
     delete ctx;
     return TW_OK;
 }
@@ -326,7 +341,27 @@ tw_status tw_ctx_synchronize(tw_ctx *ctx)
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->h2d));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->d2h));
-    return TW_OK;
+    return check_kernel_errors(ctx);
+}
+
+// Test hook, not part of the public header: sets how long the solve's CTAs
+// wait at a grid barrier on this context (0 restores the 30 s default) and
+// returns the previous value.  A test shortens it to make the bounded wait
+// give up and checks that the solve reports TW_ERR_TIMEOUT and the context
+// keeps working.
+unsigned long long tw_internal_set_solve_barrier_ns(tw_ctx *ctx, unsigned long long ns)
+{
+    if (!ctx) return 0;
+    return ctx->solve_barrier_ns.exchange(ns ? ns : 30000000000ull);
+}
+
+// Test hook, not part of the public header: turns the shared-memory staging
+// of TPS resample units on (1) or off (0) for this context and returns the
+// previous setting; off, every unit gathers its taps from global memory.
+int tw_internal_set_resample_staging(tw_ctx *ctx, int on)
+{
+    if (!ctx) return 0;
+    return ctx->resample_staging.exchange(on ? 1 : 0);
 }
 
 int64_t tw_grid_size(int64_t sz, int g) { return g > 0 && sz > 0 ? grid_size(sz, g) : -1; }
@@ -387,7 +422,10 @@ tw_status tw_warp_tps_device(tw_ctx *ctx, const void *dev_nodes, int g, int dtyp
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     RJob j = tps_job(dev_src, sz, dev_dst, sz, static_cast<const float4 *>(dev_nodes), g, dtype, interp);
     TW_TRY(run_jobs(ctx, &j, 1, st));
-    if (!stream) TW_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!stream) {
+        TW_CUDA_TRY(cudaStreamSynchronize(st));
+        return check_kernel_errors(ctx);
+    }
     return TW_OK;
 }
 

@@ -13,8 +13,9 @@ bool is_pinned_ptr(const void *p);
 
 // wait = false queues the whole solve on `st` and returns at once; the
 // solve's status is then read with solve_status(ctx, t->d_status, st).
+// h_stage: optional pinned staging for the landmark uploads (solve_tps_device).
 tw_status make_tps(tw_ctx *ctx, const tw_marker *centres, const tw_marker *values, int n, double lambda,
-                   double scale, cudaStream_t st, tw_tps **out, bool wait = true);
+                   double scale, cudaStream_t st, tw_tps **out, bool wait = true, double *h_stage = nullptr);
 void destroy_tps(tw_tps *t);
 tw_status eval_grid(tw_ctx *ctx, const tw_tps *t, const int64_t gsz[3], int g, const int64_t off[3], float4 *out,
                     cudaStream_t st);

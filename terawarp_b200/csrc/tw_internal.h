@@ -1,6 +1,7 @@
 // tw_internal.h -- shared internals of libterawarp_b200 (not installed).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -36,8 +37,11 @@ struct Error {
 // ------------------------------------------------------------- resample job
 
 // One warp job as the resample kernel sees it.  All coordinates are voxels;
-// "global" means the full subject / output volume of the job.
-struct RJob {
+// "global" means the full subject / output volume of the job.  128-byte
+// aligned because the TMA descriptor of the source buffer sits at its start
+// (64-byte alignment is the descriptor's own requirement).
+struct alignas(128) RJob {
+    CUtensorMap tmap;      // 3-D tensor map of the source buffer (x, y, z), one-row boxes (TPS staging)
     const void *src;       // source buffer, first element = global voxel src_o
     void *dst;             // output buffer, first element = global output voxel out_o
     const float4 *nodes;   // TPS node grid (DF, float4), node i at (i-1)g; null for affine
@@ -53,7 +57,8 @@ struct RJob {
     int64_t bricks[3];     // brick counts along x, y, z
     int64_t brick_begin;   // first flattened brick index of this job in its launch
     int g;                 // grid spacing (TPS)
-    int zs;                // output planes per TPS brick (divides g; set by run_jobs)
+    int zs;                // output planes per TPS work unit (divides g or is a multiple of it; set by run_jobs)
+    int tma_ok;            // tmap is valid: TPS units may stage their source footprint in shared memory
     int dtype;             // 1 u8, 2 u16
     int kind;              // 0 affine, 1 TPS
     int interp;            // 0 trilinear, 1 nearest
@@ -62,10 +67,21 @@ struct RJob {
 // Launch one resample pass over `njobs` jobs that share (dtype, kind, g).
 // jobs_dev is device memory holding the RJob array; total_bricks is the sum
 // of all jobs' bricks.  Returns a cudaError_t from the launch.
+// err: device word the kernel ORs a failure code into (a bounded wait that
+// gave up); may be null.
 cudaError_t launch_resample(const RJob *jobs_dev, int njobs, int64_t total_bricks, int dtype,
-                            int kind, int g, int interp, cudaStream_t st, int sm_count);
-// Brick extents for a (kind, g) pair.
+                            int kind, int g, int interp, cudaStream_t st, int sm_count, int *err);
+// Brick extents for a (kind, g) pair: x, y and the z extent a unit's frame
+// is anchored to (a control cell layer for TPS).
 void brick_dims(int kind, int g, int64_t out[3]);
+// Fills j.tmap / j.tma_ok for a TPS job (false when the source buffer's
+// address or pitches do not meet the TMA rules; the job then gathers).
+bool encode_source_map(RJob &j);
+// Device error word bits set by the resample kernels.
+constexpr int kKernErrTimeout = 1;
+// Source elements per TMA row copy of the staged TPS path (the tensor map's box
+// width; the staged box of a unit is at most this wide).
+constexpr int kStageBoxW = 96;
 
 // ---------------------------------------------------------------- TPS eval
 
@@ -92,9 +108,14 @@ struct SolveWork;   // device workspace of one solve
 // caller reads the status later (solve_status).  When ctr32_out and
 // coef32_out are given it also writes the FP32 evaluation arrays: centres
 // relative to `o` and the negated non-affine coefficients (-c_x, -c_y, -c_z).
+// h_stage: optional pinned host memory of at least 7n doubles that stays
+// untouched until the solve's copies have run (the caller owns it); the
+// landmark uploads then go through it instead of the context's staging ring,
+// so the host never waits for earlier work queued on `st`.
 tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
                            double *d_c_out, double *d_d_out, int *d_status_out, double *h_d_out,
-                           const double o[3], float4 *ctr32_out, float4 *coef32_out, cudaStream_t st);
+                           const double o[3], float4 *ctr32_out, float4 *coef32_out, cudaStream_t st,
+                           double *h_stage = nullptr);
 // The status word of a solve as a tw_status (waits for `st`).
 tw_status solve_status(tw_ctx *ctx, const int *d_status, cudaStream_t st);
 tw_status fit_affine_device(tw_ctx *ctx, const double *h_tar, const double *h_sub, int n, double M[16],
@@ -126,7 +147,7 @@ struct tw_ctx {
     // host staging area with its device copy.  A slot is reused once the
     // launch that last read it has completed (its event), so a launch of up
     // to kJobsPerSlot jobs needs no allocation and no host wait.
-    static constexpr int kJobSlots = 8;
+    static constexpr int kJobSlots = 32;
     static constexpr int kJobsPerSlot = 64;
     std::mutex job_mu;
     tw::RJob *job_h = nullptr;          // pinned, kJobSlots x kJobsPerSlot
@@ -141,6 +162,15 @@ struct tw_ctx {
     cudaEvent_t stage_ev[kStageSlots] = {};
     int stage_next = 0;
     std::atomic<uint64_t> launches{0};
+    int *d_err = nullptr;               // device word: kernels OR failure bits into it (kKernErrTimeout)
+    // how long a CTA of the cooperative solve waits at a grid barrier before
+    // it gives up (TW_ERR_TIMEOUT); tests shorten it through
+    // tw_internal_set_solve_barrier_ns
+    std::atomic<unsigned long long> solve_barrier_ns{30000000000ull};
+    // TPS resample units may stage their source footprint in shared memory
+    // (TMA); tests turn it off through tw_internal_set_resample_staging to
+    // compare the staged output with the gathered one
+    std::atomic<int> resample_staging{1};
     mutable std::mutex err_mu;
     std::string last_error;
 };
@@ -173,4 +203,8 @@ void dfree_on(tw_ctx *ctx, void *p, size_t bytes, cudaStream_t st);
 // copies larger than a staging slot fall back to a pageable copy.
 tw_status upload(tw_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st);
 inline void count_launch(tw_ctx *ctx, uint64_t k = 1) { if (ctx) ctx->launches += k; }
+// Reads and clears the context's device error word (call after the work that
+// may have set it has completed); TW_ERR_TIMEOUT when a kernel gave up on a
+// bounded wait.
+tw_status check_kernel_errors(tw_ctx *ctx);
 }  // namespace tw

@@ -79,15 +79,21 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
             total += jobs[i].bricks[0] * jobs[i].bricks[1] * jobs[i].bricks[2];
         }
     };
-    // TPS bricks cover one cell layer; when a launch has too few of them to
-    // fill every SM a few times, split each layer over several CTAs
-    int zs = jobs[0].kind == 1 ? jobs[0].g : 8;
+    // TPS units walk 64 output planes (several cell layers: the staged source
+    // window is loaded once per walk); when a launch has too few units to
+    // fill every SM a few times, they get shorter, down to parts of a layer
+    int zs = jobs[0].kind == 1 ? std::max(64, jobs[0].g) : 8;
     count(zs);
-    while (jobs[0].kind == 1 && zs > 1 && total < 4 * (int64_t)ctx->sm_count) {
+    while (jobs[0].kind == 1 && zs > 1 && total < 8 * (int64_t)ctx->sm_count) {
         zs /= 2;
         count(zs);
     }
     if (total == 0) return TW_OK;
+    if (jobs[0].kind == 1 && jobs[0].interp == 0)
+        for (int i = 0; i < njobs; ++i) {
+            if (ctx->resample_staging.load()) encode_source_map(jobs[i]);
+            else jobs[i].tma_ok = 0;
+        }
     const size_t bytes = sizeof(RJob) * (size_t)njobs;
     if (njobs <= tw_ctx::kJobsPerSlot && ctx->job_d) {
         // descriptors through the context's slot ring: an asynchronous copy
@@ -101,7 +107,7 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
         std::memcpy(h, jobs, bytes);
         TW_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
         cudaError_t e = launch_resample(d, njobs, total, jobs[0].dtype, jobs[0].kind, jobs[0].g, jobs[0].interp, st,
-                                        ctx->sm_count);
+                                        ctx->sm_count, ctx->d_err);
         if (e != cudaSuccess) return fail(ctx, TW_ERR_CUDA, std::string("resample launch: ") + cudaGetErrorString(e));
         TW_CUDA_TRY(cudaEventRecord(ctx->job_ev[s], st));
         count_launch(ctx);
@@ -111,11 +117,64 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
     TW_CUDA_TRY(cudaMallocAsync((void **)&d_jobs, bytes, st));
     TW_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs, bytes, cudaMemcpyHostToDevice, st));
     cudaError_t e = launch_resample(d_jobs, njobs, total, jobs[0].dtype, jobs[0].kind, jobs[0].g, jobs[0].interp, st,
-                                    ctx->sm_count);
+                                    ctx->sm_count, ctx->d_err);
     cudaFreeAsync(d_jobs, st);
     if (e != cudaSuccess) return fail(ctx, TW_ERR_CUDA, std::string("resample launch: ") + cudaGetErrorString(e));
     count_launch(ctx);
     return TW_OK;
+}
+
+// ------------------------------------------------------- TMA descriptors
+
+namespace {
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver API); null when the driver lacks it.
+EncodeTiled encode_fn()
+{
+    static EncodeTiled fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiled) nullptr;
+        }
+        return reinterpret_cast<EncodeTiled>(f);
+    }();
+    return fn;
+}
+
+}  // namespace
+
+bool encode_source_map(RJob &j)
+{
+    j.tma_ok = 0;
+    const EncodeTiled fn = encode_fn();
+    if (!fn || !j.src) return false;
+    const uint64_t es = j.dtype == TW_U8 ? 1 : 2;
+    // TMA rules: 16-byte aligned base and row / plane pitches; a box no wider
+    // than the tensor
+    if (reinterpret_cast<uintptr_t>(j.src) % 16 != 0) return false;
+    if ((j.src_py * es) % 16 != 0 || (j.src_pz * es) % 16 != 0) return false;
+    if (j.src_n[0] < kStageBoxW || j.src_n[1] < 1 || j.src_n[2] < 1) return false;
+    if (j.src_n[0] > 0xffffffffLL || j.src_n[1] > 0xffffffffLL || j.src_n[2] > 0xffffffffLL) return false;
+    if ((uint64_t)j.src_pz * es >= (1ull << 40)) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)j.src_n[0], (cuuint64_t)j.src_n[1], (cuuint64_t)j.src_n[2]};
+    const cuuint64_t strides[2] = {(cuuint64_t)j.src_py * es, (cuuint64_t)j.src_pz * es};
+    const cuuint32_t box[3] = {(cuuint32_t)kStageBoxW, 1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(&j.tmap, es == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3,
+                          const_cast<void *>(j.src), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    j.tma_ok = 1;
+    return true;
 }
 
 // ------------------------------------------------------------ sample hulls
@@ -454,7 +513,7 @@ tw_status stream_slabs(tw_ctx *ctx, const SlabIO &io,
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->d2h));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->h2d));
-    return TW_OK;
+    return check_kernel_errors(ctx);
 }
 
 }  // namespace tw

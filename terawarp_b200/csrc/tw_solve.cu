@@ -244,12 +244,12 @@ __global__ void k_fill_a(const double *__restrict__ ctr, int n, const double *__
 
 constexpr int kSolveThreads = 256;
 constexpr int kStTimeout = 4;
-// A CTA gives up on a barrier after this long (ns).  The launch is
+// A CTA gives up on a barrier after limit_ns (the context's
+// solve_barrier_ns, 30 s unless a test shortened it).  The launch is
 // cooperative, so every CTA can be resident at once; while other work (the
 // previous job's resample, a caller's kernel on another stream) still holds
 // SMs, some CTAs start later than others and the early ones wait, so the
 // bound is generous, but it is a bound.
-constexpr unsigned long long kBarrierLimitNs = 30000000000ull;
 
 struct GridBar {
     unsigned int count;   // CTAs arrived at the current barrier
@@ -268,7 +268,7 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
 // Grid-wide barrier with a bounded wait.  `gen` is the caller's count of
 // barriers passed (kept by thread 0).  Returns false, on every thread of the
 // CTA, if this or another CTA gave up; the caller then returns.
-__device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status)
+__device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status, unsigned long long limit_ns)
 {
     __shared__ int ok_sh;
     __syncthreads();
@@ -284,7 +284,7 @@ __device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status)
             const unsigned long long t0 = globaltimer_ns();
             while (*reinterpret_cast<volatile unsigned int *>(&b->gen) == g) {
                 if (*reinterpret_cast<volatile int *>(&b->err) ||
-                    globaltimer_ns() - t0 > kBarrierLimitNs) {
+                    globaltimer_ns() - t0 > limit_ns) {
                     atomicOr(&b->err, 1);
                     atomicOr(status, kStTimeout);
                     ok = 0;
@@ -502,18 +502,18 @@ __device__ void bwd_diag(const double *__restrict__ A, int m, int kb, double *__
 }
 
 __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict__ A, int m, double *__restrict__ Z,
-                                                              int *status, GridBar *bar)
+                                                              int *status, GridBar *bar, unsigned long long limit_ns)
 {
     extern __shared__ double sm[];
     unsigned int gen = 0;
     const int nblk = (m + kNB - 1) / kNB;
     if (blockIdx.x == 0) potrf_tile(A, m, 0, status, sm);
-    if (!grid_sync(bar, gen, status)) return;
+    if (!grid_sync(bar, gen, status, limit_ns)) return;
     for (int kb = 0; kb < nblk; ++kb) {
         const int rest = nblk - kb - 1;
         // row blocks below the diagonal: the rest of A plus the right-hand-side block
         for (int b = blockIdx.x; b < rest + 1; b += gridDim.x) trsm_tile(A, m, kb, kb + 1 + b, sm);
-        if (!grid_sync(bar, gen, status)) return;
+        if (!grid_sync(bar, gen, status, limit_ns)) return;
         // Lookahead: tile 0 of the trailing update is the next diagonal block
         // (kb+1, kb+1), which no other tile of this step touches; CTA 0 updates
         // it first and factors it at once, while the other CTAs are still on
@@ -523,16 +523,16 @@ __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict
             syrk_tile(A, m, kb, t, sm);
             if (t == 0 && rest > 0) potrf_tile(A, m, kb + 1, status, sm);
         }
-        if (!grid_sync(bar, gen, status)) return;
+        if (!grid_sync(bar, gen, status, limit_ns)) return;
     }
     // y' sits in rows m..m+3; back substitution L' x = y into Z rows 4..n-1
     double *z = Z + 16;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
     for (int e = gt; e < 4 * m; e += gstride) z[e] = __ldcg(&A[(size_t)(m + (e & 3)) * m + (e >> 2)]);
-    if (!grid_sync(bar, gen, status)) return;
+    if (!grid_sync(bar, gen, status, limit_ns)) return;
     for (int kb = nblk - 1; kb >= 0; --kb) {
         if (blockIdx.x == 0) bwd_diag(A, m, kb, z, sm);
-        if (!grid_sync(bar, gen, status)) return;
+        if (!grid_sync(bar, gen, status, limit_ns)) return;
         const int r0 = kb * kNB, nb = min(kNB, m - r0);
         for (int i = gt; i < r0; i += gstride) {
             double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict
             double *zi = z + i * 4;
             zi[0] = __ldcg(zi) - s0; zi[1] = __ldcg(zi + 1) - s1; zi[2] = __ldcg(zi + 2) - s2; zi[3] = __ldcg(zi + 3) - s3;
         }
-        if (!grid_sync(bar, gen, status)) return;
+        if (!grid_sync(bar, gen, status, limit_ns)) return;
     }
 }
 
@@ -736,7 +736,7 @@ struct StreamBuf {
 
 tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val, int n, double lambda,
                            double *d_c_out, double *d_d_out, int *d_status_out, double *h_d_out, const double o[3],
-                           float4 *ctr32_out, float4 *coef32_out, cudaStream_t st)
+                           float4 *ctr32_out, float4 *coef32_out, cudaStream_t st, double *h_stage)
 {
     const int m = n - 4;
     // workspace: ctr 3n, Y 4n, Xw 4n, V 4n, P 4n, W 4n, Z 4n, KC 4n, tau 4, R 16, d 16, status
@@ -774,8 +774,15 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
         hY[4 * i + 2] = h_val[3 * i + 1];
         hY[4 * i + 3] = h_val[3 * i + 2];
     }
-    TW_TRY(upload(ctx, d_ctr, h_ctr, sizeof(double) * 3 * n, st));
-    TW_TRY(upload(ctx, d_Y, hY.data(), sizeof(double) * 4 * n, st));
+    if (h_stage) {
+        std::memcpy(h_stage, h_ctr, sizeof(double) * 3 * n);
+        std::memcpy(h_stage + 3 * (size_t)n, hY.data(), sizeof(double) * 4 * n);
+        TW_CUDA_TRY(cudaMemcpyAsync(d_ctr, h_stage, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+        TW_CUDA_TRY(cudaMemcpyAsync(d_Y, h_stage + 3 * (size_t)n, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, st));
+    } else {
+        TW_TRY(upload(ctx, d_ctr, h_ctr, sizeof(double) * 3 * n, st));
+        TW_TRY(upload(ctx, d_Y, hY.data(), sizeof(double) * 4 * n, st));
+    }
     TW_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     TW_CUDA_TRY(cudaMemsetAsync(d_d, 0, sizeof(double) * 16, st));
 
@@ -797,7 +804,8 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
         if (per_sm < 1) return fail(ctx, TW_ERR_CUDA, "solve kernel does not fit on an SM");
         int grid = ctx->sm_count;
         TW_CUDA_TRY(cudaMemsetAsync(d_bar, 0, sizeof(GridBar), st));
-        void *args[] = {(void *)&d_A, (void *)&m, (void *)&d_Z, (void *)&d_status, (void *)&d_bar};
+        unsigned long long limit_ns = ctx->solve_barrier_ns.load();
+        void *args[] = {(void *)&d_A, (void *)&m, (void *)&d_Z, (void *)&d_status, (void *)&d_bar, (void *)&limit_ns};
         TW_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_chol_solve, dim3(grid), dim3(kSolveThreads), args,
                                                 kSolveSmem, st));
         ++nl;

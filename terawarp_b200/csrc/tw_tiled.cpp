@@ -44,11 +44,25 @@ struct Slot {
     void *d_src = nullptr, *d_dst = nullptr;
     void *h_src = nullptr, *h_dst = nullptr;
     cudaEvent_t e_in = nullptr, e_comp = nullptr, e_out = nullptr;
-    int64_t tile = -1;       // tile whose result is in flight in this slot
+    int64_t batch = -1;      // batch whose result is in flight in this slot
 };
 
-// Source-box bound for a tile from the hull of its sample positions.
-Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3])
+// Tiles warped by one resample launch: a full tile goes alone; the smaller
+// ones (the volume's uneven edge tiles) are grouped, in tile order, until a
+// group holds as many output voxels as a full tile (at most 64 tiles).  Each
+// tile's source box and output sit in the slot's buffers at 256-byte aligned
+// element offsets.
+struct Batch {
+    std::vector<int64_t> tiles;
+    std::vector<int64_t> src_off, out_off;
+    int64_t src_total = 0, out_total = 0;
+};
+
+// Source-box bound for a tile from the hull of its sample positions.  With
+// align > 1 the box's x extent is widened (inside the volume) to a multiple of
+// `align` elements and to at least min_x, so that its rows meet the TMA rules
+// of the staged resample (16-byte pitches, rows no narrower than one copy).
+Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3], int64_t align = 1, int64_t min_x = 0)
 {
     Box b;
     for (int a = 0; a < 3; ++a) {
@@ -63,6 +77,13 @@ Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3])
         h = std::min<int64_t>(h, sz[a] - 1);
         b.o[a] = l;
         b.n[a] = h >= l ? h - l + 1 : 0;
+    }
+    if (align > 1 && b.n[0] > 0 && b.n[1] > 0 && b.n[2] > 0) {
+        int64_t w = std::max(b.n[0], std::min(min_x, sz[0]));
+        w = std::min(sz[0], ((w + align - 1) / align) * align);
+        const int64_t o = std::max<int64_t>(0, std::min(b.o[0], sz[0] - w));
+        b.o[0] = o;
+        b.n[0] = w;
     }
     return b;
 }
@@ -96,9 +117,9 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
         if (opts->staging_depth > 0) depth = std::min(4, std::max(2, opts->staging_depth));
     }
     if (kind == 1) {
-        // TPS tiles start on resample-brick boundaries of the whole volume
-        // (256 in x, max(g, 8) in y, a control cell in z): every brick then has
-        // the origin it has in a whole-volume warp, so the tiled output equals
+        // TPS tiles start on resample-unit boundaries of the whole volume
+        // (64 in x, 16 in y, a control cell layer in z): every unit then has
+        // the frame it has in a whole-volume warp, so the tiled output equals
         // the whole-volume output voxel for voxel
         int64_t bd[3];
         brick_dims(1, g, bd);
@@ -129,7 +150,8 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
         const int64_t gsz[3] = {grid_size(out_sz[0], g), grid_size(out_sz[1], g), grid_size(out_sz[2], g)};
         std::vector<float> lo, hi;
         TW_TRY(tps_box_hull(ctx, nodes, gsz, g, cb, ctx->stream, lo, hi));
-        for (int64_t t = 0; t < ntiles; ++t) srcs[t] = box_from_hull(&lo[3 * t], &hi[3 * t], src_sz);
+        for (int64_t t = 0; t < ntiles; ++t)
+            srcs[t] = box_from_hull(&lo[3 * t], &hi[3 * t], src_sz, 16 / (int64_t)es, kStageBoxW);
     } else {
         for (int64_t t = 0; t < ntiles; ++t) {
             float lo[3], hi[3];
@@ -149,10 +171,44 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
             srcs[t] = box_from_hull(lo, hi, src_sz);
         }
     }
+    // batches: every full tile alone, then the edge tiles in groups
+    const int64_t full = T[0] * T[1] * T[2];
+    std::vector<Batch> batches;
+    auto align_up = [&](int64_t v) {
+        const int64_t q = 256 / (int64_t)es;
+        return (v + q - 1) / q * q;
+    };
+    auto add = [&](Batch &b, int64_t t) {
+        b.tiles.push_back(t);
+        b.src_off.push_back(b.src_total);
+        b.out_off.push_back(b.out_total);
+        b.src_total += align_up(srcs[t].count());
+        b.out_total += align_up(tiles[t].count());
+    };
+    for (int64_t t = 0; t < ntiles; ++t)
+        if (tiles[t].count() == full) {
+            batches.emplace_back();
+            add(batches.back(), t);
+        }
+    {
+        Batch b;
+        int64_t out = 0;
+        for (int64_t t = 0; t < ntiles; ++t) {
+            if (tiles[t].count() == full) continue;
+            if (!b.tiles.empty() && (out + tiles[t].count() > full || (int64_t)b.tiles.size() >= tw_ctx::kJobsPerSlot)) {
+                batches.push_back(std::move(b));
+                b = Batch();
+                out = 0;
+            }
+            add(b, t);
+            out += tiles[t].count();
+        }
+        if (!b.tiles.empty()) batches.push_back(std::move(b));
+    }
     int64_t max_src = 1, max_out = 1;
-    for (int64_t t = 0; t < ntiles; ++t) {
-        max_src = std::max(max_src, srcs[t].count());
-        max_out = std::max(max_out, tiles[t].count());
+    for (const Batch &b : batches) {
+        max_src = std::max(max_src, b.src_total);
+        max_out = std::max(max_out, b.out_total);
     }
 
     // the built-in host-volume reader/writer on pinned memory become DMA copies
@@ -197,51 +253,64 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
         TW_CUDA_TRY(cudaEventCreateWithFlags(&s.e_out, cudaEventDisableTiming));
     }
 
-    // hands a finished tile to the sink (after its D2H completed)
+    // hands a finished batch's tiles to the sink (after their D2H completed)
     auto retire = [&](Slot &s) -> tw_status {
-        if (s.tile < 0) return TW_OK;
+        if (s.batch < 0) return TW_OK;
         TW_CUDA_TRY(cudaEventSynchronize(s.e_out));
-        const Box &b = tiles[s.tile];
+        const Batch &bt = batches[s.batch];
         if (!dma_out && io.write) {
-            if (io.write(io.write_user, b.o[0], b.o[1], b.o[2], b.n[0], b.n[1], b.n[2], s.h_dst) != 0)
-                return fail(ctx, TW_ERR_IO, "tile sink failed at tile " + std::to_string(s.tile));
+            for (size_t i = 0; i < bt.tiles.size(); ++i) {
+                const int64_t t = bt.tiles[i];
+                const Box &b = tiles[t];
+                const char *h = static_cast<const char *>(s.h_dst) + (size_t)bt.out_off[i] * es;
+                if (io.write(io.write_user, b.o[0], b.o[1], b.o[2], b.n[0], b.n[1], b.n[2], h) != 0)
+                    return fail(ctx, TW_ERR_IO, "tile sink failed at tile " + std::to_string(t));
+            }
         }
-        s.tile = -1;
+        s.batch = -1;
         return TW_OK;
     };
 
-    for (int64_t t = 0; t < ntiles; ++t) {
-        Slot &s = slots[t % depth];
+    std::vector<RJob> jobs;
+    for (int64_t bi = 0; bi < (int64_t)batches.size(); ++bi) {
+        Slot &s = slots[bi % depth];
         TW_TRY(retire(s));  // frees the slot's pinned output and, transitively, its device buffers
-        const Box &tb = tiles[t];
-        const Box &sb = srcs[t];
-        const bool empty = sb.count() == 0;
-        // 1. source box -> device slot
-        if (!empty) {
+        const Batch &bt = batches[bi];
+        // 1. source boxes -> device slot
+        for (size_t i = 0; i < bt.tiles.size(); ++i) {
+            const int64_t t = bt.tiles[i];
+            const Box &sb = srcs[t];
+            if (sb.count() == 0) continue;
+            char *d = static_cast<char *>(s.d_src) + (size_t)bt.src_off[i] * es;
             const int64_t zero[3] = {0, 0, 0};
             if (dma_in) {
-                TW_CUDA_TRY(copy_box(s.d_src, hv_in->data, sb.n[0], sb.n[1], zero, hv_in->sz[0], hv_in->sz[1], sb.o,
-                                     sb.n, es, cudaMemcpyHostToDevice, ctx->h2d));
+                TW_CUDA_TRY(copy_box(d, hv_in->data, sb.n[0], sb.n[1], zero, hv_in->sz[0], hv_in->sz[1], sb.o, sb.n,
+                                     es, cudaMemcpyHostToDevice, ctx->h2d));
             } else {
                 if (!io.read) return fail(ctx, TW_ERR_ARG, "no tile source");
-                if (io.read(io.read_user, sb.o[0], sb.o[1], sb.o[2], sb.n[0], sb.n[1], sb.n[2], s.h_src) != 0)
+                char *h = static_cast<char *>(s.h_src) + (size_t)bt.src_off[i] * es;
+                if (io.read(io.read_user, sb.o[0], sb.o[1], sb.o[2], sb.n[0], sb.n[1], sb.n[2], h) != 0)
                     return fail(ctx, TW_ERR_IO, "tile source failed at tile " + std::to_string(t));
-                TW_CUDA_TRY(cudaMemcpyAsync(s.d_src, s.h_src, (size_t)sb.count() * es, cudaMemcpyHostToDevice,
-                                            ctx->h2d));
+                TW_CUDA_TRY(cudaMemcpyAsync(d, h, (size_t)sb.count() * es, cudaMemcpyHostToDevice, ctx->h2d));
             }
         }
         TW_CUDA_TRY(cudaEventRecord(s.e_in, ctx->h2d));
-        // 2. warp the tile (or zero it when no sample can land in the volume)
+        // 2. warp the batch's tiles in one launch (tiles no sample of which
+        // lands in the volume are zeroed instead)
         TW_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, s.e_in, 0));
-        if (empty) {
-            TW_CUDA_TRY(cudaMemsetAsync(s.d_dst, 0, (size_t)tb.count() * es, ctx->stream));
-        } else {
-            RJob j;
-            if (kind == 1) {
-                j = tps_job(s.d_src, src_sz, s.d_dst, out_sz, nodes, g, dtype, interp);
-            } else {
-                j = affine_job(s.d_src, src_sz, s.d_dst, out_sz, M, dtype, interp);
+        jobs.clear();
+        for (size_t i = 0; i < bt.tiles.size(); ++i) {
+            const int64_t t = bt.tiles[i];
+            const Box &tb = tiles[t];
+            const Box &sb = srcs[t];
+            char *dd = static_cast<char *>(s.d_dst) + (size_t)bt.out_off[i] * es;
+            if (sb.count() == 0) {
+                TW_CUDA_TRY(cudaMemsetAsync(dd, 0, (size_t)tb.count() * es, ctx->stream));
+                continue;
             }
+            const char *ds = static_cast<const char *>(s.d_src) + (size_t)bt.src_off[i] * es;
+            RJob j = kind == 1 ? tps_job(ds, src_sz, dd, out_sz, nodes, g, dtype, interp)
+                               : affine_job(ds, src_sz, dd, out_sz, M, dtype, interp);
             for (int a = 0; a < 3; ++a) {
                 j.src_o[a] = sb.o[a];
                 j.src_n[a] = sb.n[a];
@@ -252,27 +321,35 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
             j.src_pz = sb.n[0] * sb.n[1];
             j.dst_py = tb.n[0];
             j.dst_pz = tb.n[0] * tb.n[1];
-            TW_TRY(run_jobs(ctx, &j, 1, ctx->stream));
+            jobs.push_back(j);
         }
+        if (!jobs.empty()) TW_TRY(run_jobs(ctx, jobs.data(), (int)jobs.size(), ctx->stream));
         TW_CUDA_TRY(cudaEventRecord(s.e_comp, ctx->stream));
-        // 3. tile -> host (retire() has already waited for this slot's
-        // previous tile, so its buffers are free for the next use)
+        // 3. tiles -> host (retire() has already waited for this slot's
+        // previous batch, so its buffers are free for the next use)
         TW_CUDA_TRY(cudaStreamWaitEvent(ctx->d2h, s.e_comp, 0));
         const int64_t zero[3] = {0, 0, 0};
-        if (dma_out) {
-            TW_CUDA_TRY(copy_box(hv_out->data, s.d_dst, hv_out->sz[0], hv_out->sz[1], tb.o, tb.n[0], tb.n[1], zero,
-                                 tb.n, es, cudaMemcpyDeviceToHost, ctx->d2h));
-        } else {
-            TW_CUDA_TRY(cudaMemcpyAsync(s.h_dst, s.d_dst, (size_t)tb.count() * es, cudaMemcpyDeviceToHost, ctx->d2h));
+        for (size_t i = 0; i < bt.tiles.size(); ++i) {
+            const int64_t t = bt.tiles[i];
+            const Box &tb = tiles[t];
+            const char *dd = static_cast<const char *>(s.d_dst) + (size_t)bt.out_off[i] * es;
+            if (dma_out) {
+                TW_CUDA_TRY(copy_box(hv_out->data, dd, hv_out->sz[0], hv_out->sz[1], tb.o, tb.n[0], tb.n[1], zero,
+                                     tb.n, es, cudaMemcpyDeviceToHost, ctx->d2h));
+            } else {
+                char *h = static_cast<char *>(s.h_dst) + (size_t)bt.out_off[i] * es;
+                TW_CUDA_TRY(cudaMemcpyAsync(h, dd, (size_t)tb.count() * es, cudaMemcpyDeviceToHost, ctx->d2h));
+            }
         }
         TW_CUDA_TRY(cudaEventRecord(s.e_out, ctx->d2h));
-        s.tile = t;
+        s.batch = bi;
     }
-    for (int64_t t = std::max<int64_t>(0, ntiles - depth); t < ntiles; ++t) TW_TRY(retire(slots[t % depth]));
+    const int64_t nb = (int64_t)batches.size();
+    for (int64_t bi = std::max<int64_t>(0, nb - depth); bi < nb; ++bi) TW_TRY(retire(slots[bi % depth]));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->h2d));
     TW_CUDA_TRY(cudaStreamSynchronize(ctx->d2h));
-    return TW_OK;
+    return check_kernel_errors(ctx);
 }
 
 void copy_rows(char *dst, const char *src, int64_t nrows, size_t row_bytes, int64_t dst_pitch, int64_t src_pitch,

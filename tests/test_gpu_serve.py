@@ -89,3 +89,34 @@ def test_many_small_jobs_complete(ctx):
             srv.wait(i)
     for v, o in zip(vols, outs):
         np.testing.assert_array_equal(o, O.affine_warp(v, M))
+
+
+def test_device_resident_jobs_equal_alone_results_and_report_stage_times(ctx):
+    """Jobs whose volumes already live in HBM are warped in place (no copy);
+    each result equals the job run alone, and every job reports its stage
+    times in order."""
+    jobs = synth.serving_jobs(24, seed=91, dims_lo=(64, 48, 32), dims_hi=(192, 160, 64), n_lo=8, n_hi=300, g=8)
+    vols = [make_volume(j.shape_zyx, j.dtype, 200 + i) for i, j in enumerate(jobs)]
+    d_src = [torch.from_numpy(v).cuda() for v in vols]
+    d_out = [torch.empty_like(x) for x in d_src]
+    with api.Server(ctx, max_inflight=8) as srv:
+        ids = []
+        for j, s, o in zip(jobs, d_src, d_out):
+            if j.kind == "tps":
+                ids.append(srv.submit_tps(j.centres, j.values, j.g, s, o))
+            else:
+                ids.append(srv.submit_affine(j.M, s, o))
+        for i in ids:
+            srv.wait(i)
+        times = [srv.job_times(i) for i in ids]
+    torch.cuda.synchronize()
+    for j, v, o in zip(jobs, vols, d_out):
+        np.testing.assert_array_equal(o.cpu().numpy(), run_alone(ctx, j, v), err_msg=f"{j.kind} {j.shape_zyx}")
+    for j, t in zip(jobs, times):
+        assert t["latency"] > 0 and t["queued"] >= 0
+        assert t["ready"] is not None and t["resample_start"] is not None
+        assert t["resample_end"] >= t["resample_start"] >= 0 and t["done"] >= t["resample_end"]
+        if j.kind == "tps":
+            assert t["solve"] is not None and t["grid"] >= t["solve"]
+        else:
+            assert t["solve"] is None and t["grid"] is None

@@ -29,11 +29,9 @@ def case():
 def test_tiled_tps_equals_whole_volume(ctx, case):
     img, sub, tar = case
     whole = tw.imgwarp_smallmemory_image(ctx, sub, tar, 8, 8, 8, 1, 0, img)
-    # same node grid and per-voxel arithmetic; only the frame origins of the
-    # FP32 sample positions can differ (bricks split differently per launch)
+    # same node grid, the same unit frames and the same per-voxel arithmetic
     tiled = api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, 8, img, tile=(256, 256, 64), depth=2)
-    d = agree(tiled, whole)
-    assert (d == 0).mean() >= 0.999
+    np.testing.assert_array_equal(tiled, whole)
 
 
 def test_tiled_tps_uneven_tiles_and_pinned_dma(ctx, case):
@@ -115,4 +113,25 @@ def test_autotuned_tile_choice_gives_the_whole_volume_result(ctx):
     assert (tile, depth) in [(t, d) for t, d in cands] and len(table) == 3
     tiled = api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, 8, vol, tile=tile, depth=depth)
     whole = tw.imgwarp_smallmemory_image(ctx, sub, tar, 8, 8, 8, 1, 0, vol)
+    np.testing.assert_array_equal(tiled, whole)
+
+
+def test_edge_tiles_are_batched_and_equal_the_whole_volume(ctx, case):
+    """Uneven edge tiles are warped in shared launches (fewer resample launches
+    than tiles) and the tiled result equals the whole-volume result voxel for
+    voxel: tiles start on the whole volume's resample-unit boundaries."""
+    img, sub, tar = case                     # 520 x 300 x 96 u16, g = 8
+    whole = tw.imgwarp_smallmemory_image(ctx, sub, tar, 8, 8, 8, 1, 0, img)
+    # launches of one solve + node grid, to subtract from the tiled call's count
+    n0 = ctx.kernel_launches
+    t = tw.tps_solve(ctx, tar, sub)
+    solve_launches = ctx.kernel_launches - n0
+    t.close()
+    before = ctx.kernel_launches
+    tiled = api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, 8, img, tile=(256, 128, 64), depth=2)
+    resample_launches = ctx.kernel_launches - before - solve_launches - 2  # node grid + tile hulls
+    # tiles: x 256, 256, 8; y 128, 128, 44; z 64, 32 -> 18 tiles, 4 of them full
+    ntiles, nfull = 18, 4
+    assert resample_launches < ntiles
+    assert resample_launches >= nfull + 1
     np.testing.assert_array_equal(tiled, whole)
