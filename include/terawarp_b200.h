@@ -64,6 +64,9 @@ const char *tw_status_string(tw_status s);
 int tw_abi_version(void);
 /* Number of kernels this context has launched (counter for benchmarks). */
 uint64_t tw_ctx_kernel_launches(const tw_ctx *ctx);
+/* Bytes the context's streaming paths (whole-volume slabs, tiled engine)
+ * have copied host -> device and device -> host (counters for benchmarks). */
+void tw_ctx_transfer_bytes(const tw_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 /* Blocks until all work queued on the context's streams has finished. */
 tw_status tw_ctx_synchronize(tw_ctx *ctx);
 
@@ -231,13 +234,43 @@ int tw_box_reader_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t n
 int tw_box_writer_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
                        const void *src);
 
+/* A procedural volume for running the tiled path at terabyte scale with no
+ * stored volume: every voxel is a function of its coordinates and the seed
+ * (hash noise 0..10, Gaussian blobs, short random-walk fibres), so any two
+ * boxes agree where they overlap.  threads: host threads per box (0 = all). */
+typedef struct {
+    uint64_t seed;
+    int64_t sz[3];
+    int dtype;
+    int threads;
+} tw_synthetic_volume;
+/* tw_read_box_fn over a tw_synthetic_volume (user = tw_synthetic_volume*). */
+int tw_box_reader_synthetic(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                            void *dst);
+
+/* A sink that keeps only a checksum of what it receives: the sum of the
+ * voxel values, a position-weighted sum (a tile written to the wrong place
+ * changes it), and the voxel count.  Zero-initialise before use. */
+typedef struct {
+    uint64_t sum, weighted, voxels;
+    int dtype;
+    int threads;
+} tw_checksum;
+/* tw_write_box_fn over a tw_checksum (user = tw_checksum*). */
+int tw_box_writer_checksum(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz,
+                           const void *src);
+
 typedef struct {
     int64_t tile[3];        /* output tile dims x, y, z (0 = 512; reference:    */
                             /* 1000^3); TPS tiles are rounded down to whole     */
-                            /* resample bricks (256 x max(g,8) x g), at least   */
-                            /* one brick                                        */
+                            /* resample units (64 x 16 x g), at least one unit  */
     int staging_depth;      /* tiles in flight, 2..4 (0 = 2: double buffering)  */
     int interp;             /* tw_interp                                        */
+    int64_t region_o[3];    /* output region to warp: [region_o, region_o +     */
+    int64_t region_n[3];    /* region_n) (all region_n 0 = the whole output);   */
+                            /* the sink receives only tiles of it.  A TPS       */
+                            /* region grows to whole resample units (64 x 16 x  */
+                            /* g voxels of the output grid)                     */
 } tw_tile_opts;
 
 /* Mirror of imgwarp_smallmemory_CYF (q_imgwarp_tps_quicksmallmemory.h:86-87,

@@ -24,8 +24,18 @@ class tw_host_volume(C.Structure):
     _fields_ = [("data", C.c_void_p), ("sz", C.c_int64 * 3), ("dtype", C.c_int), ("threads", C.c_int)]
 
 
+class tw_synthetic_volume(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("sz", C.c_int64 * 3), ("dtype", C.c_int), ("threads", C.c_int)]
+
+
+class tw_checksum(C.Structure):
+    _fields_ = [("sum", C.c_uint64), ("weighted", C.c_uint64), ("voxels", C.c_uint64), ("dtype", C.c_int),
+                ("threads", C.c_int)]
+
+
 class tw_tile_opts(C.Structure):
-    _fields_ = [("tile", C.c_int64 * 3), ("staging_depth", C.c_int), ("interp", C.c_int)]
+    _fields_ = [("tile", C.c_int64 * 3), ("staging_depth", C.c_int), ("interp", C.c_int),
+                ("region_o", C.c_int64 * 3), ("region_n", C.c_int64 * 3)]
 
 
 class tw_params(C.Structure):
@@ -65,6 +75,7 @@ SIGNATURES = {
     "tw_status_string": (C.c_char_p, [C.c_int]),
     "tw_abi_version": (C.c_int, []),
     "tw_ctx_kernel_launches": (C.c_uint64, [_P]),
+    "tw_ctx_transfer_bytes": (None, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "tw_ctx_synchronize": (C.c_int, [_P]),
     "tw_tps_solve": (C.c_int, [_P, _MP, _MP, C.c_int, C.c_double, C.POINTER(_P)]),
     "tw_tps_destroy": (C.c_int, [_P]),
@@ -92,6 +103,9 @@ SIGNATURES = {
     "tw_bigimagewarp": (C.c_int, [_P, C.POINTER(tw_params), _MP, _MP, C.c_int, C.c_int, _P, _I64P, _P]),
     "tw_downsample_factor": (C.c_int, [_I64P]),
     "tw_downsample_image": (C.c_int, [_P, C.c_int, _P, _I64P, _P, _I64P]),
+    "tw_box_reader_synthetic": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                          _P]),
+    "tw_box_writer_checksum": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
     "tw_v3draw_read_header": (C.c_int, [C.c_char_p, _I64P, C.POINTER(C.c_int), _I64P]),
     "tw_v3draw_read": (C.c_int, [C.c_char_p, _P, C.c_size_t]),
     "tw_v3draw_read_box": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,

@@ -146,6 +146,13 @@ class Context:
     def kernel_launches(self) -> int:
         return int(self.lib.tw_ctx_kernel_launches(self.handle))
 
+    @property
+    def transfer_bytes(self):
+        """(host -> device, device -> host) bytes the streaming paths moved."""
+        a, b = C.c_uint64(), C.c_uint64()
+        self.lib.tw_ctx_transfer_bytes(self.handle, C.byref(a), C.byref(b))
+        return int(a.value), int(b.value)
+
     def synchronize(self) -> None:
         _check(self.lib.tw_ctx_synchronize(self.handle), self, "tw_ctx_synchronize")
 
@@ -279,13 +286,65 @@ def q_imagewarp_affine_image(ctx: Context, ql_marker_tar, ql_marker_sub, p_img_s
     return out
 
 
-def _tile_opts(tile, depth, interp) -> L.tw_tile_opts:
+def _tile_opts(tile, depth, interp, region=None) -> L.tw_tile_opts:
     o = L.tw_tile_opts()
     for a in range(3):
         o.tile[a] = int(tile[a]) if tile is not None else 0
     o.staging_depth = int(depth)
     o.interp = int(interp)
+    if region is not None:
+        (ox, oy, oz), (nx, ny, nz) = region
+        for a, (ov, nv) in enumerate(((ox, nx), (oy, ny), (oz, nz))):
+            o.region_o[a] = int(ov)
+            o.region_n[a] = int(nv)
     return o
+
+
+class SyntheticVolume:
+    """A procedural tile source (tw_synthetic_volume): voxels from a seeded
+    hash of their coordinates, no storage; shape (z, y, x)."""
+
+    def __init__(self, shape_zyx, dtype, seed: int = 1, threads: int = 0):
+        self.v = L.tw_synthetic_volume()
+        self.v.seed = int(seed)
+        self.v.sz[0], self.v.sz[1], self.v.sz[2] = int(shape_zyx[2]), int(shape_zyx[1]), int(shape_zyx[0])
+        self.dtype_code = L.TW_U8 if np.dtype(dtype) == np.uint8 else L.TW_U16
+        self.v.dtype = self.dtype_code
+        self.v.threads = int(threads)
+        self.shape = tuple(int(s) for s in shape_zyx)
+        self.shape_xyz = (self.shape[2], self.shape[1], self.shape[0])
+        self.dtype = np.dtype(dtype)
+        self.handle = C.cast(C.pointer(self.v), C.c_void_p)
+
+    def read_box(self, o_xyz, n_xyz) -> np.ndarray:
+        nx, ny, nz = (int(v) for v in n_xyz)
+        a = np.empty((nz, ny, nx), self.dtype)
+        rc = L.load().tw_box_reader_synthetic(self.handle, int(o_xyz[0]), int(o_xyz[1]), int(o_xyz[2]), nx, ny, nz,
+                                              a.ctypes.data)
+        if rc != 0:
+            raise TeraWarpError(L.TW_ERR_IO, f"synthetic read failed ({rc})")
+        return a
+
+
+class Checksum:
+    """A sink that keeps the sum, a position-weighted sum and the voxel count
+    of what it receives (tw_checksum)."""
+
+    def __init__(self, dtype, threads: int = 0):
+        self.c = L.tw_checksum()
+        self.c.dtype = L.TW_U8 if np.dtype(dtype) == np.uint8 else L.TW_U16
+        self.c.threads = int(threads)
+        self.handle = C.cast(C.pointer(self.c), C.c_void_p)
+
+    def write_box(self, o_xyz, block) -> None:
+        b = np.ascontiguousarray(block)
+        nz, ny, nx = b.shape
+        L.load().tw_box_writer_checksum(self.handle, int(o_xyz[0]), int(o_xyz[1]), int(o_xyz[2]), nx, ny, nz,
+                                        b.ctypes.data)
+
+    @property
+    def value(self):
+        return int(self.c.sum), int(self.c.weighted), int(self.c.voxels)
 
 
 def _host_volume(x) -> L.tw_host_volume:
@@ -311,6 +370,9 @@ def _box_io(src, dst, read_fn=None, write_fn=None):
     if isinstance(src, SliceDir):
         rd = L.READ_BOX(C.cast(lib.tw_box_reader_slices, C.c_void_p).value)
         ru = src.handle
+    elif isinstance(src, SyntheticVolume):
+        rd = L.READ_BOX(C.cast(lib.tw_box_reader_synthetic, C.c_void_p).value)
+        ru = src.handle
     elif read_fn is None:
         hv_in = _host_volume(src)
         keep.append(hv_in)
@@ -330,6 +392,9 @@ def _box_io(src, dst, read_fn=None, write_fn=None):
         ru = None
     if isinstance(dst, SliceWriter):
         wr = L.WRITE_BOX(C.cast(lib.tw_box_writer_slices, C.c_void_p).value)
+        wu = dst.handle
+    elif isinstance(dst, Checksum):
+        wr = L.WRITE_BOX(C.cast(lib.tw_box_writer_checksum, C.c_void_p).value)
         wu = dst.handle
     elif write_fn is None:
         hv_out = _host_volume(dst)
@@ -353,26 +418,28 @@ def _box_io(src, dst, read_fn=None, write_fn=None):
 
 
 def _src_dtype(src) -> int:
-    return src.dtype_code if isinstance(src, SliceDir) else _dtype_code(src)
+    return src.dtype_code if isinstance(src, (SliceDir, SyntheticVolume)) else _dtype_code(src)
 
 
 def _src_sz3(src):
-    if isinstance(src, SliceDir):
+    if isinstance(src, (SliceDir, SyntheticVolume)):
         return (C.c_int64 * 3)(*src.shape_xyz)
     return _sz3(src)
 
 
 def imgwarp_smallmemory_tiled(ctx: Context, ql_marker_tar, ql_marker_sub, marker_scale: float, g: int, src, out=None,
-                              tile=(512, 512, 512), depth: int = 2, interp: int = 0, read_fn=None, write_fn=None):
+                              tile=(512, 512, 512), depth: int = 2, interp: int = 0, read_fn=None, write_fn=None,
+                              region=None):
     """Mirror of imgwarp_smallmemory_CYF for volumes streamed tile by tile
     (the source may exceed HBM): centres = ql_marker_sub, values =
-    ql_marker_tar, both scaled by marker_scale.  src: a host array, or a
-    SliceDir; out: a host array, or a SliceWriter."""
+    ql_marker_tar, both scaled by marker_scale.  src: a host array, a
+    SliceDir or a SyntheticVolume; out: a host array, a SliceWriter or a
+    Checksum.  region: ((x0, y0, z0), (nx, ny, nz)) of the output to warp."""
     if out is None and write_fn is None:
         out = _like(src, tuple(src.shape))
     n = _pair_count(ql_marker_tar, ql_marker_sub, "imgwarp_smallmemory_tiled")
     rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
-    opts = _tile_opts(tile, depth, interp)
+    opts = _tile_opts(tile, depth, interp, region)
     _check(ctx.lib.tw_imgwarp_smallmemory_tiled(ctx.handle, _markers(ql_marker_tar), _markers(ql_marker_sub), n,
                                                 marker_scale, g, _src_dtype(src), _src_sz3(src), rd, ru, wr, wu,
                                                 C.byref(opts)), ctx, "tw_imgwarp_smallmemory_tiled")
@@ -381,14 +448,14 @@ def imgwarp_smallmemory_tiled(ctx: Context, ql_marker_tar, ql_marker_sub, marker
 
 
 def warp_affine_tiled(ctx: Context, M, src, out_shape_zyx=None, out=None, tile=(512, 512, 512), depth: int = 2,
-                      interp: int = 0, read_fn=None, write_fn=None):
+                      interp: int = 0, read_fn=None, write_fn=None, region=None):
     """Affine warp streamed tile by tile (q_imagewarp_affine_cyf)."""
     shape = tuple(out_shape_zyx) if out_shape_zyx is not None else tuple(src.shape)
     if out is None and write_fn is None:
         out = _like(src, shape)
     Mx = np.ascontiguousarray(np.asarray(M, np.float64).reshape(16))
     rd, ru, wr, wu, keep = _box_io(src, out, read_fn, write_fn)
-    opts = _tile_opts(tile, depth, interp)
+    opts = _tile_opts(tile, depth, interp, region)
     osz = (C.c_int64 * 3)(shape[2], shape[1], shape[0])
     _check(ctx.lib.tw_warp_affine_tiled(ctx.handle, Mx.ctypes.data_as(L._DP), _src_dtype(src), _src_sz3(src), osz, rd,
                                         ru, wr, wu, C.byref(opts)), ctx, "tw_warp_affine_tiled")
@@ -534,6 +601,7 @@ def bigimagewarp_files(ctx: Context, img_sub: str, marker_sub: str, marker_tar: 
     """The plugin's command on files (tw_bigimagewarp_files): a .v3draw file or
     a directory of slices in, <name><suffix>.v3draw or <name><suffix>_slice/
     out (keyword arguments as `params`)."""
+    kw.setdefault("marker_scale", 0.0)  # 0: the reference's choice (1 for a .v3draw, 4 for slices)
     p = params(**kw)
     p.downsample_mode = int(downsample_mode)
     _check(ctx.lib.tw_bigimagewarp_files(ctx.handle, C.byref(p), str(img_sub).encode(),

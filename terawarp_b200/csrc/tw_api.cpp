@@ -334,6 +334,12 @@ const char *tw_ctx_last_error(const tw_ctx *ctx)
 
 uint64_t tw_ctx_kernel_launches(const tw_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
 
+void tw_ctx_transfer_bytes(const tw_ctx *ctx, uint64_t *h2d, uint64_t *d2h)
+{
+    if (h2d) *h2d = ctx ? ctx->h2d_bytes.load() : 0;
+    if (d2h) *d2h = ctx ? ctx->d2h_bytes.load() : 0;
+}
+
 tw_status tw_ctx_synchronize(tw_ctx *ctx)
 {
     if (!ctx) return TW_ERR_ARG;

@@ -162,6 +162,7 @@ struct tw_ctx {
     cudaEvent_t stage_ev[kStageSlots] = {};
     int stage_next = 0;
     std::atomic<uint64_t> launches{0};
+    std::atomic<uint64_t> h2d_bytes{0}, d2h_bytes{0};  // streamed by the slab and tile paths
     int *d_err = nullptr;               // device word: kernels OR failure bits into it (kKernErrTimeout)
     // how long a CTA of the cooperative solve waits at a grid barrier before
     // it gives up (TW_ERR_TIMEOUT); tests shorten it through

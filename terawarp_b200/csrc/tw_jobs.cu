@@ -479,6 +479,7 @@ tw_status stream_slabs(tw_ctx *ctx, const SlabIO &io,
                 up_slot_owner[slot] = k;
             }
             TW_CUDA_TRY(cudaEventRecord(ev_up.ev[k], ctx->h2d));
+            ctx->h2d_bytes += bytes;
             ++uploaded;
         }
         if (need_chunk >= 0) TW_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ev_up.ev[need_chunk], 0));
@@ -507,6 +508,7 @@ tw_status stream_slabs(tw_ctx *ctx, const SlabIO &io,
                 pending_down.push_back(s);
             }
             TW_CUDA_TRY(cudaEventRecord(ev_down.ev[s], ctx->d2h));
+            ctx->d2h_bytes += (size_t)(z1 - z0) * io.dst_plane_bytes;
         }
     }
     while (!pending_down.empty()) TW_TRY(drain_one());

@@ -126,18 +126,37 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
         for (int a = 0; a < 3; ++a) T[a] = std::max<int64_t>(bd[a], (T[a] / bd[a]) * bd[a]);
     }
     for (int a = 0; a < 3; ++a) T[a] = std::min(T[a], out_sz[a]);
-    int64_t nt[3];
-    for (int a = 0; a < 3; ++a) nt[a] = (out_sz[a] + T[a] - 1) / T[a];
+    // output region (the whole output unless the options name one); a TPS
+    // region grows to whole resample units so that every unit keeps its
+    // whole-volume frame
+    int64_t r0[3] = {0, 0, 0}, r1[3] = {out_sz[0], out_sz[1], out_sz[2]};
+    if (opts && (opts->region_n[0] > 0 || opts->region_n[1] > 0 || opts->region_n[2] > 0)) {
+        int64_t bd[3] = {1, 1, 1};
+        if (kind == 1) brick_dims(1, g, bd);
+        for (int a = 0; a < 3; ++a) {
+            if (opts->region_n[a] <= 0 || opts->region_o[a] < 0 || opts->region_o[a] >= out_sz[a])
+                return fail(ctx, TW_ERR_ARG, "tile region outside the output volume");
+            r0[a] = (opts->region_o[a] / bd[a]) * bd[a];
+            r1[a] = std::min(out_sz[a], ((opts->region_o[a] + opts->region_n[a] + bd[a] - 1) / bd[a]) * bd[a]);
+        }
+    }
+    int64_t nt[3], t0[3];
+    for (int a = 0; a < 3; ++a) {
+        t0[a] = r0[a] / T[a];
+        nt[a] = (r1[a] + T[a] - 1) / T[a] - t0[a];
+    }
     const int64_t ntiles = nt[0] * nt[1] * nt[2];
 
-    // tile boxes and their source footprints
+    // tile boxes (clipped to the region) and their source footprints
     std::vector<Box> tiles(ntiles), srcs(ntiles);
     for (int64_t t = 0; t < ntiles; ++t) {
         int64_t ix = t % nt[0], iy = (t / nt[0]) % nt[1], iz = t / (nt[0] * nt[1]);
-        const int64_t idx[3] = {ix, iy, iz};
+        const int64_t idx[3] = {ix + t0[0], iy + t0[1], iz + t0[2]};
         for (int a = 0; a < 3; ++a) {
-            tiles[t].o[a] = idx[a] * T[a];
-            tiles[t].n[a] = std::min(T[a], out_sz[a] - tiles[t].o[a]);
+            const int64_t lo = std::max(idx[a] * T[a], r0[a]);
+            const int64_t hi = std::min((idx[a] + 1) * T[a], r1[a]);
+            tiles[t].o[a] = lo;
+            tiles[t].n[a] = hi - lo;
         }
     }
     if (kind == 1) {
@@ -294,6 +313,7 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
                 TW_CUDA_TRY(cudaMemcpyAsync(d, h, (size_t)sb.count() * es, cudaMemcpyHostToDevice, ctx->h2d));
             }
         }
+        for (int64_t t : bt.tiles) ctx->h2d_bytes += (uint64_t)srcs[t].count() * es;
         TW_CUDA_TRY(cudaEventRecord(s.e_in, ctx->h2d));
         // 2. warp the batch's tiles in one launch (tiles no sample of which
         // lands in the volume are zeroed instead)
@@ -341,6 +361,7 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
                 TW_CUDA_TRY(cudaMemcpyAsync(h, dd, (size_t)tb.count() * es, cudaMemcpyDeviceToHost, ctx->d2h));
             }
         }
+        for (int64_t t : bt.tiles) ctx->d2h_bytes += (uint64_t)tiles[t].count() * es;
         TW_CUDA_TRY(cudaEventRecord(s.e_out, ctx->d2h));
         s.batch = bi;
     }
