@@ -289,6 +289,32 @@ tw_status tw_imgwarp_smallmemory_tiled(tw_ctx *ctx, const tw_marker *ql_marker_t
                                        tw_write_box_fn write_box, void *write_user,
                                        const tw_tile_opts *opts);
 
+/* A (tile shape, staging depth) candidate of the tiled TPS path and the time
+ * the tuner measured for it (seconds; filled in by tw_tune_tiled_tps). */
+typedef struct {
+    int64_t tile[3];
+    int staging_depth;
+    double seconds;
+} tw_tile_candidate;
+
+/* Chooses the tile shape and staging depth of tw_imgwarp_smallmemory_tiled
+ * for one job by timing the candidates (cands/ncands, or a built-in list when
+ * cands is NULL; times are written back into cands) on the job's corner block
+ * (sample dims x, y, z; 0 = 1024 x 1024 x 512, clipped to the volume): the
+ * job's own landmarks are solved and its node grid evaluated once, then each
+ * candidate streams the sample through the tiled engine from read_box into a
+ * sink that discards it.  The choice is remembered per (volume dims, dtype,
+ * g, landmark-count power-of-two bucket, device name) for the process, and
+ * in cache_path when it is given (a text file of "key tx ty tz depth seconds"
+ * lines, the last line of a key winning).  best receives the chosen tile and
+ * depth (interp 0, whole volume).  With ctx NULL only the cache file is
+ * consulted (TW_ERR_NOT_READY on a miss).  No counterpart in the reference,
+ * whose tiles are 1000^3 (q_imgwarp_tps_quicksmallmemory.cpp:1264). */
+tw_status tw_tune_tiled_tps(tw_ctx *ctx, const tw_marker *ql_marker_tar, const tw_marker *ql_marker_sub, int n,
+                            double marker_scale, int g, int dtype, const int64_t sz[3], tw_read_box_fn read_box,
+                            void *read_user, tw_tile_candidate *cands, int ncands, const int64_t sample[3],
+                            const char *cache_path, tw_tile_opts *best);
+
 /* Mirror of q_imagewarp_affine_cyf (q_warp_affine_tps.h:72, body :851-1329)
  * for an arbitrary matrix: output dims out_sz, tiles streamed as above. */
 tw_status tw_warp_affine_tiled(tw_ctx *ctx, const double M[16], int dtype, const int64_t src_sz[3],

@@ -38,6 +38,10 @@ class tw_tile_opts(C.Structure):
                 ("region_o", C.c_int64 * 3), ("region_n", C.c_int64 * 3)]
 
 
+class tw_tile_candidate(C.Structure):
+    _fields_ = [("tile", C.c_int64 * 3), ("staging_depth", C.c_int), ("seconds", C.c_double)]
+
+
 class tw_params(C.Structure):
     _fields_ = [
         ("warp_mode", C.c_int), ("device_mode", C.c_int), ("resize_mode", C.c_int), ("deformation_mode", C.c_int),
@@ -96,6 +100,9 @@ SIGNATURES = {
                                                READ_BOX, _P, WRITE_BOX, _P, C.POINTER(tw_tile_opts)]),
     "tw_warp_affine_tiled": (C.c_int, [_P, _DP, C.c_int, _I64P, _I64P, READ_BOX, _P, WRITE_BOX, _P,
                                        C.POINTER(tw_tile_opts)]),
+    "tw_tune_tiled_tps": (C.c_int, [_P, _MP, _MP, C.c_int, C.c_double, C.c_int, C.c_int, _I64P, READ_BOX, _P,
+                                    C.POINTER(tw_tile_candidate), C.c_int, _I64P, C.c_char_p,
+                                    C.POINTER(tw_tile_opts)]),
     "tw_box_reader_host": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
     "tw_box_writer_host": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P]),
     "tw_params_default": (None, [C.POINTER(tw_params)]),

@@ -1,30 +1,23 @@
-"""Autotuner for the out-of-core tiled warps.
+"""Tile-shape / staging-depth choice for the out-of-core tiled TPS warp.
 
-The tiled engine (tw_imgwarp_smallmemory_tiled / tw_warp_affine_tiled) takes
-an output tile shape and a staging depth (device/pinned slots in flight).  The
-best pair depends on the volume, the voxel type, the grid spacing and the
-host-device link, so it is chosen by timing a few candidates on a sample of
-the job -- the corner block of the output, warped with the job's own
-landmarks -- and remembered per (kind, volume shape, dtype, grid spacing,
-landmark-count bucket, device name).
-
-`tune(run, candidates)` is the search itself: `run(tile_xyz, depth)` returns
-seconds, the fastest candidate wins.
+The tuner itself is in the library (tw_tune_tiled_tps): it solves the job's
+landmarks and evaluates its node grid once, times each candidate (tile
+shape, staging depth) on the job's corner block through the tiled engine,
+and remembers the winner per (volume dims, dtype, grid spacing, landmark
+count rounded up to a power of two, device name) for the process and, when
+a cache file is given, across processes.  This module is its Python caller.
 """
 from __future__ import annotations
 
-import json
-import math
-import os
-import time
-from pathlib import Path
-from typing import Callable, Iterable, Sequence
+import ctypes as C
 
 import numpy as np
 
-# (tile x, y, z), staging depth.  TPS tiles are rounded to the grid spacing by
-# the engine.  Flat tiles move fewer halo voxels per output voxel in z-major
-# volumes; deeper staging hides more of the link.
+from . import _lib as L
+
+# The library's default candidates: (tile x, y, z), staging depth.  TPS tiles
+# are rounded to whole resample units by the engine.  Flat tiles move fewer
+# halo voxels per output voxel; deeper staging hides more of the link.
 CANDIDATES: list[tuple[tuple[int, int, int], int]] = [
     ((512, 512, 512), 2),
     ((512, 512, 512), 3),
@@ -35,98 +28,51 @@ CANDIDATES: list[tuple[tuple[int, int, int], int]] = [
 ]
 
 
-def tune(run: Callable[[tuple, int], float], candidates: Iterable = CANDIDATES, repeats: int = 1):
-    """Times every candidate (best of `repeats`) and returns
-    (tile_xyz, depth, table) with table = [(tile_xyz, depth, seconds), ...]."""
-    table = []
-    for tile, depth in candidates:
-        best = math.inf
-        for _ in range(max(1, repeats)):
-            best = min(best, float(run(tuple(tile), int(depth))))
-        table.append((tuple(int(v) for v in tile), int(depth), best))
-    if not table:
-        raise ValueError("no candidates to tune over")
-    tile, depth, _ = min(table, key=lambda r: r[2])
-    return tile, depth, table
-
-
-def cache_key(kind: str, shape_zyx: Sequence[int], dtype: str, g: int = 0, n_landmarks: int = 0,
-              device: str = "") -> str:
-    """Landmark counts fall into power-of-two buckets (the solve and the node
-    evaluation scale with them, the tile choice only coarsely)."""
-    bucket = 0 if n_landmarks <= 0 else 1 << int(math.ceil(math.log2(n_landmarks)))
-    z, y, x = (int(v) for v in shape_zyx)
-    return f"{kind}:{x}x{y}x{z}:{dtype}:g{int(g)}:n{bucket}:{device}"
-
-
-def load_cache(path) -> dict:
-    try:
-        return json.loads(Path(path).read_text())
-    except (OSError, ValueError):
-        return {}
-
-
-def store_cache(path, key: str, tile, depth: int, table) -> None:
-    p = Path(path)
-    data = load_cache(p)
-    data[key] = {"tile": list(tile), "depth": int(depth),
-                 "table": [[list(t), int(d), float(s)] for t, d, s in table]}
-    p.parent.mkdir(parents=True, exist_ok=True)
-    tmp = p.with_suffix(p.suffix + ".tmp")
-    tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
-    os.replace(tmp, p)
-
-
-def _sample(src, sample_zyx):
-    """Contiguous copy of the source's corner block (pinned when torch)."""
-    z, y, x = (min(int(a), int(b)) for a, b in zip(sample_zyx, src.shape))
-    crop = src[:z, :y, :x]
-    try:
-        import torch
-        if isinstance(crop, torch.Tensor):
-            out = torch.empty(tuple(crop.shape), dtype=crop.dtype, pin_memory=True)
-            out.copy_(crop)
-            return out
-    except ImportError:
-        pass
-    return np.ascontiguousarray(crop)
-
-
-def _empty_like(x):
-    try:
-        import torch
-        if isinstance(x, torch.Tensor):
-            return torch.empty(tuple(x.shape), dtype=x.dtype, pin_memory=True)
-    except ImportError:
-        pass
-    return np.empty_like(x)
+def _cands(candidates):
+    arr = (L.tw_tile_candidate * len(candidates))()
+    for i, (tile, depth) in enumerate(candidates):
+        for a in range(3):
+            arr[i].tile[a] = int(tile[a])
+        arr[i].staging_depth = int(depth)
+    return arr
 
 
 def tune_tiled_tps(ctx, ql_marker_tar, ql_marker_sub, marker_scale: float, g: int, src,
-                   sample_zyx=(512, 1024, 1024), candidates=CANDIDATES, cache_path=None, device_name: str = ""):
+                   sample_zyx=(512, 1024, 1024), candidates=CANDIDATES, cache_path=None):
     """(tile_xyz, depth, table) for imgwarp_smallmemory_tiled on `src` (a host
-    volume z, y, x), timed on its corner block; cached when cache_path is set."""
+    volume z, y, x or a SliceDir); table = [(tile_xyz, depth, seconds)] of the
+    candidates timed now (empty when the choice came from a cache)."""
     from . import api
 
     candidates = list(candidates)
-    dtype = "u8" if np.dtype(str(src.dtype).replace("torch.", "")).itemsize == 1 else "u16"
-    n = len(np.asarray(ql_marker_tar).reshape(-1, 3))
-    key = cache_key("tps", src.shape, dtype, g, n, device_name)
-    if cache_path:
-        hit = load_cache(cache_path).get(key)
-        if hit:
-            return tuple(hit["tile"]), int(hit["depth"]), [(tuple(t), d, s) for t, d, s in hit["table"]]
-    crop = _sample(src, sample_zyx)
-    out = _empty_like(crop)
+    n = api._pair_count(ql_marker_tar, ql_marker_sub, "tune_tiled_tps")
+    rd, ru, _, _, keep = api._box_io(src, None, None, lambda *a: None)
+    arr = _cands(candidates)
+    best = L.tw_tile_opts()
+    smp = (C.c_int64 * 3)(int(sample_zyx[2]), int(sample_zyx[1]), int(sample_zyx[0]))
+    st = L.load().tw_tune_tiled_tps(ctx.handle if ctx is not None else None, api._markers(ql_marker_tar),
+                                    api._markers(ql_marker_sub), n, float(marker_scale), int(g), api._src_dtype(src),
+                                    api._src_sz3(src), rd, ru, arr, len(candidates), smp,
+                                    str(cache_path).encode() if cache_path else None, C.byref(best))
+    del keep
+    api._check(st, ctx, "tw_tune_tiled_tps")
+    tile = tuple(int(best.tile[a]) for a in range(3))
+    table = [(tuple(int(arr[i].tile[a]) for a in range(3)), int(arr[i].staging_depth), float(arr[i].seconds))
+             for i in range(len(candidates)) if arr[i].seconds > 0]
+    return tile, int(best.staging_depth), table
 
-    def run(tile, depth):
-        t0 = time.perf_counter()
-        api.imgwarp_smallmemory_tiled(ctx, ql_marker_tar, ql_marker_sub, marker_scale, g, crop, out=out, tile=tile,
-                                      depth=depth)
-        return time.perf_counter() - t0
 
-    run(candidates[0][0], candidates[0][1])  # the first call pays one-time set-up
-    tile, depth, table = tune(run, candidates)
-    if cache_path:
-        store_cache(cache_path, key, tile, depth, table)
-    return tile, depth, table
+def cached_choice(shape_zyx, dtype, g: int, n_landmarks: int, cache_path):
+    """The cached (tile_xyz, depth) for a job from the cache file alone (no
+    GPU, device name empty), or None."""
+    best = L.tw_tile_opts()
+    z, y, x = (int(v) for v in shape_zyx)
+    sz = (C.c_int64 * 3)(x, y, z)
+    code = L.TW_U8 if np.dtype(dtype) == np.uint8 else L.TW_U16
+    st = L.load().tw_tune_tiled_tps(None, None, None, int(n_landmarks), 1.0, int(g), code, sz, L.READ_BOX(0), None,
+                                    None, 0, None, str(cache_path).encode(), C.byref(best))
+    if st == L.TW_ERR_NOT_READY:
+        return None
+    if st != L.TW_OK:
+        raise RuntimeError(f"tw_tune_tiled_tps: status {st}")
+    return tuple(int(best.tile[a]) for a in range(3)), int(best.staging_depth)

@@ -15,9 +15,15 @@
 #include "tw_host.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -392,9 +398,142 @@ void copy_rows(char *dst, const char *src, int64_t nrows, size_t row_bytes, int6
     for (auto &x : th) x.join();
 }
 
+// ------------------------------------------------------------- autotuner
+
+std::mutex g_tune_mu;
+std::map<std::string, tw_tile_candidate> g_tune_cache;  // choices made in this process
+
+std::string tune_key(const int64_t sz[3], int dtype, int g, int n, const std::string &device)
+{
+    int64_t bucket = 0;
+    if (n > 0)
+        for (bucket = 1; bucket < n; bucket <<= 1) {
+        }
+    std::ostringstream k;
+    k << "tps:" << sz[0] << "x" << sz[1] << "x" << sz[2] << ":" << (dtype == TW_U8 ? "u8" : "u16") << ":g" << g
+      << ":n" << bucket << ":" << device;
+    return k.str();
+}
+
+bool cache_file_lookup(const char *path, const std::string &key, tw_tile_candidate &out)
+{
+    std::ifstream f(path);
+    if (!f) return false;
+    bool found = false;
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream in(line);
+        std::string k;
+        tw_tile_candidate c{};
+        if (in >> k >> c.tile[0] >> c.tile[1] >> c.tile[2] >> c.staging_depth >> c.seconds && k == key) {
+            out = c;
+            found = true;  // the last line of a key wins
+        }
+    }
+    return found;
+}
+
+void cache_file_store(const char *path, const std::string &key, const tw_tile_candidate &c)
+{
+    std::ofstream f(path, std::ios::app);
+    if (f) f << key << " " << c.tile[0] << " " << c.tile[1] << " " << c.tile[2] << " " << c.staging_depth << " "
+             << c.seconds << "\n";
+}
+
+// A sink that discards the tiles (the tuner times the pipeline, not a sink).
+int discard_box(void *, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, const void *) { return 0; }
+
 }  // namespace
 
 extern "C" {
+
+tw_status tw_tune_tiled_tps(tw_ctx *ctx, const tw_marker *ql_marker_tar, const tw_marker *ql_marker_sub, int n,
+                            double marker_scale, int g, int dtype, const int64_t sz[3], tw_read_box_fn read_box,
+                            void *read_user, tw_tile_candidate *cands, int ncands, const int64_t sample[3],
+                            const char *cache_path, tw_tile_opts *best)
+{
+    if (!sz || !best || (dtype != TW_U8 && dtype != TW_U16) || !g_supported(g)) return TW_ERR_ARG;
+    std::string device;
+    if (ctx) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) return fail(ctx, TW_ERR_CUDA, "device query");
+        device = prop.name;
+        for (char &ch : device)
+            if (ch == ' ') ch = '_';
+    }
+    const std::string key = tune_key(sz, dtype, g, n, device);
+    auto give = [&](const tw_tile_candidate &c) {
+        std::memset(best, 0, sizeof(*best));
+        for (int a = 0; a < 3; ++a) best->tile[a] = c.tile[a];
+        best->staging_depth = c.staging_depth;
+        return TW_OK;
+    };
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return give(it->second);
+    }
+    tw_tile_candidate hit{};
+    if (cache_path && cache_file_lookup(cache_path, key, hit)) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = hit;
+        return give(hit);
+    }
+    if (!ctx) return TW_ERR_NOT_READY;
+    if (!ql_marker_tar || !ql_marker_sub || n < 4 || !read_box) return fail(ctx, TW_ERR_ARG, "tuning needs the job's landmarks and source");
+    static const tw_tile_candidate kDefault[] = {
+        {{512, 512, 512}, 2, 0}, {{512, 512, 512}, 3, 0}, {{1024, 1024, 256}, 2, 0},
+        {{1024, 1024, 256}, 3, 0}, {{2048, 1024, 128}, 3, 0}, {{256, 256, 256}, 4, 0}};
+    std::vector<tw_tile_candidate> list;
+    if (cands && ncands > 0) list.assign(cands, cands + ncands);
+    else list.assign(kDefault, kDefault + sizeof(kDefault) / sizeof(kDefault[0]));
+    TW_CUDA_TRY(cudaSetDevice(ctx->device));
+    // the job's field, once: solve + node grid of the whole volume
+    tw_tps *tp = nullptr;
+    TW_TRY(make_tps(ctx, ql_marker_sub, ql_marker_tar, n, 0.2, marker_scale > 0 ? marker_scale : 1.0, ctx->stream, &tp));
+    std::unique_ptr<tw_tps, void (*)(tw_tps *)> guard(tp, destroy_tps);
+    const int64_t gsz[3] = {grid_size(sz[0], g), grid_size(sz[1], g), grid_size(sz[2], g)};
+    void *nodes = nullptr;
+    const size_t nbytes = sizeof(float4) * (size_t)(gsz[0] * gsz[1] * gsz[2]);
+    TW_TRY(dmalloc(ctx, &nodes, nbytes));
+    struct NodeGuard {
+        tw_ctx *c; void *p; size_t b;
+        ~NodeGuard() { cudaStreamSynchronize(c->stream); dfree(c, p, b); }
+    } ng{ctx, nodes, nbytes};
+    const int64_t off[3] = {0, 0, 0};
+    TW_TRY(eval_grid(ctx, tp, gsz, g, off, static_cast<float4 *>(nodes), ctx->stream));
+    const int64_t sdef[3] = {1024, 1024, 512};
+    TileIO io{read_box, read_user, discard_box, nullptr};
+    auto time_one = [&](const tw_tile_candidate &c, double &secs) -> tw_status {
+        tw_tile_opts o;
+        std::memset(&o, 0, sizeof(o));
+        for (int a = 0; a < 3; ++a) {
+            o.tile[a] = c.tile[a];
+            o.region_o[a] = 0;
+            o.region_n[a] = std::min(sz[a], sample && sample[a] > 0 ? sample[a] : sdef[a]);
+        }
+        o.staging_depth = c.staging_depth;
+        const auto t0 = std::chrono::steady_clock::now();
+        TW_TRY(run_tiled(ctx, 1, static_cast<const float4 *>(nodes), g, nullptr, dtype, 0, sz, sz, io, &o));
+        secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return TW_OK;
+    };
+    double warm = 0;
+    TW_TRY(time_one(list[0], warm));  // the first run pays one-time set-up
+    size_t bi = 0;
+    for (size_t i = 0; i < list.size(); ++i) {
+        TW_TRY(time_one(list[i], list[i].seconds));
+        if (list[i].seconds < list[bi].seconds) bi = i;
+    }
+    if (cands && ncands > 0)
+        for (int i = 0; i < ncands; ++i) cands[i].seconds = list[(size_t)i].seconds;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = list[bi];
+    }
+    if (cache_path) cache_file_store(cache_path, key, list[bi]);
+    return give(list[bi]);
+}
 
 int tw_box_reader_host(void *user, int64_t x0, int64_t y0, int64_t z0, int64_t nx, int64_t ny, int64_t nz, void *dst)
 {

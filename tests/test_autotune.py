@@ -1,58 +1,39 @@
-"""Autotuner search and cache (host logic; the GPU timing itself is exercised
-by the bench's tiled leg)."""
-import json
-
-import pytest
+"""The tiled autotuner's cache (tw_tune_tiled_tps consulted without a
+context: CPU only).  Choices are keyed by volume dims, dtype, grid spacing,
+the landmark count rounded up to a power of two, and the device name; the
+last line of a key in the cache file wins."""
+import numpy as np
 
 from terawarp_b200 import autotune
 
 
-def test_tune_picks_the_fastest_candidate_best_of_repeats():
-    calls = []
-    times = {((512, 512, 512), 2): [0.30, 0.20], ((1024, 1024, 256), 3): [0.25, 0.26], ((256, 256, 256), 4): [0.5, 0.4]}
-
-    def run(tile, depth):
-        k = (tile, depth)
-        calls.append(k)
-        return times[k][sum(1 for c in calls if c == k) - 1]
-
-    tile, depth, table = autotune.tune(run, list(times), repeats=2)
-    assert (tile, depth) == ((512, 512, 512), 2)  # best-of-2: 0.20 beats 0.25
-    assert [t[2] for t in table] == [0.20, 0.25, 0.4]
-    assert len(calls) == 6
+def write_cache(path, lines):
+    path.write_text("".join(l + "\n" for l in lines))
 
 
-def test_tune_rejects_an_empty_candidate_list():
-    with pytest.raises(ValueError):
-        autotune.tune(lambda t, d: 1.0, [])
+def test_cached_choice_from_the_file(tmp_path):
+    p = tmp_path / "tune.txt"
+    write_cache(p, ["tps:256x128x64:u16:g16:n128: 256 128 64 3 0.01",
+                    "tps:256x128x64:u8:g16:n128: 128 128 64 2 0.02"])
+    assert autotune.cached_choice((64, 128, 256), np.uint16, 16, 100, p) == ((256, 128, 64), 3)
+    assert autotune.cached_choice((64, 128, 256), np.uint8, 16, 100, p) == ((128, 128, 64), 2)
 
 
-def test_cache_key_buckets_landmark_counts():
-    k1 = autotune.cache_key("tps", (512, 2048, 2048), "u16", 16, 1500, "B200")
-    k2 = autotune.cache_key("tps", (512, 2048, 2048), "u16", 16, 2000, "B200")
-    k3 = autotune.cache_key("tps", (512, 2048, 2048), "u16", 16, 2049, "B200")
-    assert k1 == k2 != k3
-    assert k1 == "tps:2048x2048x512:u16:g16:n2048:B200"
+def test_landmark_counts_share_a_power_of_two_bucket(tmp_path):
+    p = tmp_path / "tune.txt"
+    write_cache(p, ["tps:2048x2048x512:u16:g16:n2048: 1024 1024 256 3 0.5"])
+    assert autotune.cached_choice((512, 2048, 2048), np.uint16, 16, 1500, p) == ((1024, 1024, 256), 3)
+    assert autotune.cached_choice((512, 2048, 2048), np.uint16, 16, 2048, p) == ((1024, 1024, 256), 3)
+    assert autotune.cached_choice((512, 2048, 2048), np.uint16, 16, 2049, p) is None
+    assert autotune.cached_choice((512, 2048, 2048), np.uint16, 8, 2000, p) is None
 
 
-def test_cache_round_trip(tmp_path):
-    p = tmp_path / "sub" / "autotune.json"
-    assert autotune.load_cache(p) == {}
-    table = [((512, 512, 512), 2, 0.2), ((1024, 1024, 256), 3, 0.25)]
-    autotune.store_cache(p, "k", (512, 512, 512), 2, table)
-    autotune.store_cache(p, "k2", (1024, 1024, 256), 3, table)
-    data = json.loads(p.read_text())
-    assert data["k"]["tile"] == [512, 512, 512] and data["k"]["depth"] == 2
-    assert data["k2"]["table"][1] == [[1024, 1024, 256], 3, 0.25]
-
-
-def test_tune_tiled_tps_returns_a_cached_choice_without_running(tmp_path):
-    import numpy as np
-    src = np.zeros((64, 128, 256), np.uint16)
-    tar = np.zeros((100, 3), np.float32)
-    key = autotune.cache_key("tps", src.shape, "u16", 16, 100, "B200")
-    path = tmp_path / "a.json"
-    autotune.store_cache(path, key, (256, 128, 64), 3, [((256, 128, 64), 3, 0.01)])
-    tile, depth, table = autotune.tune_tiled_tps(None, tar, tar, 1.0, 16, src, cache_path=path, device_name="B200")
-    assert (tile, depth) == ((256, 128, 64), 3)
-    assert table == [((256, 128, 64), 3, 0.01)]
+def test_last_line_of_a_key_wins_and_misses_report_none(tmp_path):
+    p = tmp_path / "tune.txt"
+    write_cache(p, ["tps:64x64x64:u16:g8:n16: 64 64 64 2 0.3",
+                    "tps:64x64x64:u16:g8:n16: 64 64 32 4 0.2"])
+    assert autotune.cached_choice((64, 64, 64), np.uint16, 8, 16, p) == ((64, 64, 32), 4)
+    assert autotune.cached_choice((64, 64, 65), np.uint16, 8, 16, p) is None
+    # a choice once made is remembered by the process, file or not
+    assert autotune.cached_choice((64, 64, 64), np.uint16, 8, 16, tmp_path / "absent.txt") == ((64, 64, 32), 4)
+    assert autotune.cached_choice((96, 64, 64), np.uint16, 8, 16, tmp_path / "absent.txt") is None
