@@ -302,9 +302,13 @@ __device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status, unsigned l
     return ok_sh != 0;
 }
 
-// potrf of diagonal block kb in shared memory: in step j threads j..63 take
-// the pivot (x rsqrt(d)) and scale column j, then each thread updates its 4 x 4
-// patch of the trailing lower triangle from register copies of the column.
+// potrf of diagonal block kb in shared memory, by one warp: lane l owns rows
+// l and l + 32.  In step j the owners of rows below j scale their element of
+// column j by rsqrt(pivot) and keep it in a register, then update their rows'
+// elements of the trailing lower triangle, column by column, from that
+// register and the (broadcast) scaled element of the column's own row.  The
+// warp synchronises with __syncwarp only, so a block costs no CTA barriers
+// beyond the two around it (the other warps wait there).
 __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, double *sm)
 {
     double(*a)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
@@ -318,40 +322,30 @@ __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, d
         a[r][c] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
     }
     __syncthreads();
-    const int t = threadIdx.x;
-    // thread t updates rows tr + 16u and columns tc + 16v of the block: the
-    // 16 threads of a half-warp then read 16 consecutive rows of a column
-    // (distinct banks with the 65-double row pitch)
-    const int tr = t >> 4, tc = t & 15;
-    for (int j = 0; j < kNB; ++j) {
-        if (t >= j && t < kNB) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const int i0 = lane, i1 = lane + 32;
+        for (int j = 0; j < kNB; ++j) {
             double d = a[j][j];
             if (!(d > 0.0)) {
-                if (t == j) atomicOr(status, kStNotSPD);
+                if (lane == 0) atomicOr(status, kStNotSPD);
                 d = 1.0;
             }
             const double inv = rsqrt(d);
-            if (t == j) sd[j] = d * inv;
-            else a[t][j] *= inv;
-        }
-        __syncthreads();
-        if (tr + 48 > j) {
-            double ci[4], cl[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                ci[u] = a[tr + 16 * u][j];
-                cl[u] = a[tc + 16 * u][j];
+            double c0 = 0.0, c1 = 0.0;
+            if (i0 > j) { c0 = a[i0][j] * inv; a[i0][j] = c0; }
+            if (i1 > j) { c1 = a[i1][j] * inv; a[i1][j] = c1; }
+            if (lane == 0) sd[j] = d * inv;
+            __syncwarp();
+            for (int l = j + 1; l < kNB; ++l) {
+                const double cl = a[l][j];
+                if (i0 >= l) a[i0][l] -= c0 * cl;
+                if (i1 >= l) a[i1][l] -= c1 * cl;
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const int i = tr + 16 * u, l = tc + 16 * v;
-                    if (l > j && i >= l) a[i][l] -= ci[u] * cl[v];
-                }
+            __syncwarp();
         }
-        __syncthreads();
     }
+    __syncthreads();
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
         if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c < r ? a[r][c] : (c == r ? sd[r] : 0.0);
@@ -359,14 +353,15 @@ __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, d
 }
 
 // trsm of row block ib against diagonal block kb: L(ib,kb) = A(ib,kb) L(kb,kb)^-T.
-// Thread (r, q) keeps row r's columns q, q+4, .. in registers; column c is
-// finished by its owner (x 1/L(c,c)), broadcast through shared memory, and
-// subtracted from the later columns: X(r,c') -= X(r,c) L(c',c).
+// Rows are independent: the four lanes (q = lane & 3) of one row keep its
+// columns q, q+4, .. in registers; column c is finished by its owner (x
+// 1/L(c,c)), handed to the other three by a warp shuffle, and subtracted from
+// the later columns: X(r,c') -= X(r,c) L(c',c).  No CTA barrier inside the
+// column loop.
 __device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double *sm)
 {
     double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
     double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
-    double(*xs)[kNB] = reinterpret_cast<double(*)[kNB]>(sm + 2 * kNB * (kNB + 1));
     double *rdiag = sm + 2 * kNB * (kNB + 1) + 2 * kNB;
     const int nblk = (m + kNB - 1) / kNB;
     const int r0 = kb * kNB;
@@ -382,25 +377,22 @@ __device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double 
     }
     __syncthreads();
     if (threadIdx.x < kNB) rdiag[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
-    const int r = threadIdx.x & (kNB - 1);
-    const int q = threadIdx.x >> 6;
+    const int lane = threadIdx.x & 31;
+    const int r = (threadIdx.x >> 5) * 8 + (lane >> 2);  // 8 rows per warp
+    const int q = lane & 3;
+    const int base = lane & ~3;
     double x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = X[r][4 * k + q];
-    __syncthreads();  // X is rewritten below as columns finish
+    __syncthreads();  // rdiag is visible
     // fully unrolled so that every index into x is a constant (x stays in
     // registers); columns at or beyond nbk are skipped
 #pragma unroll
     for (int c = 0; c < kNB; ++c) {
         if (c >= nbk) break;
-        if (q == (c & 3)) {
-            // the finished column goes straight to X (it is not updated again)
-            const double own = x[c >> 2] * rdiag[c];
-            X[r][c] = own;
-            xs[c & 1][r] = own;
-        }
-        __syncthreads();
-        const double xc = xs[c & 1][r];
+        const double mine = x[c >> 2] * rdiag[c];           // meaningful in the owner lane only
+        const double xc = __shfl_sync(0xffffffffu, mine, base | (c & 3));
+        if (q == (c & 3)) X[r][c] = xc;
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             const int cp = 4 * k + q;
