@@ -453,7 +453,9 @@ class _RingAlloc:
     def take(self, nbytes: int, job_key) -> int:
         if nbytes > self.n:
             raise ValueError("job larger than the output ring")
-        start = self.head if self.head + nbytes <= self.n else 0
+        # slices start on 256-byte boundaries (any voxel type, aligned DMA)
+        head = (self.head + 255) & ~255
+        start = head if head + nbytes <= self.n else 0
         end = start + nbytes
         keep = []
         for (k, a, b) in self.live:

@@ -54,6 +54,22 @@ def _ptr(x) -> int:
     raise TypeError(f"unsupported buffer type {type(x)}")
 
 
+def _stream_arg(stream, *bufs) -> int:
+    """The stream handle for a device call.  With no stream the library runs
+    the call on the context's own stream and returns when it is complete;
+    work that torch has queued on its current stream for these tensors
+    (their producers) is finished first, since the context's stream is not
+    ordered after torch's."""
+    if stream:
+        return int(stream)
+    import torch
+    for b in bufs:
+        if _is_torch(b) and b.is_cuda:
+            torch.cuda.current_stream(b.device).synchronize()
+            break
+    return 0
+
+
 def _dtype_code(x) -> int:
     if _is_torch(x):
         import torch
@@ -203,7 +219,7 @@ def tps_eval_grid(ctx: Context, tps: TPS, gsz: Sequence[int], g: int, offset=(0,
     if out is None:
         out = torch.empty((gz, gy, gx, 4), dtype=torch.float32, device=f"cuda:{ctx.device}")
     _check(ctx.lib.tw_tps_eval_grid(ctx.handle, tps.handle, gx, gy, gz, g, int(offset[0]), int(offset[1]),
-                                    int(offset[2]), C.c_void_p(_ptr(out)), C.c_void_p(stream or 0)),
+                                    int(offset[2]), C.c_void_p(_ptr(out)), C.c_void_p(_stream_arg(stream, out))),
            ctx, "tw_tps_eval_grid")
     return out
 
@@ -212,7 +228,7 @@ def warp_tps_device(ctx: Context, nodes, g: int, src, dst, interp: int = 0, stre
     """Fused B-spline + resample of device volumes (z, y, x)."""
     _check(ctx.lib.tw_warp_tps_device(ctx.handle, C.c_void_p(_ptr(nodes)), g, _dtype_code(src), interp,
                                       C.c_void_p(_ptr(src)), C.c_void_p(_ptr(dst)), _sz3(src),
-                                      C.c_void_p(stream or 0)), ctx, "tw_warp_tps_device")
+                                      C.c_void_p(_stream_arg(stream, nodes, src, dst))), ctx, "tw_warp_tps_device")
 
 
 def fit_affine(ctx: Context, tar, sub) -> np.ndarray:
@@ -253,7 +269,7 @@ def warp_affine_device(ctx: Context, M, src, dst, interp: int = 0, stream=None) 
     Mx = np.ascontiguousarray(np.asarray(M, np.float64).reshape(16))
     _check(ctx.lib.tw_warp_affine_device(ctx.handle, Mx.ctypes.data_as(L._DP), _dtype_code(src), interp,
                                          C.c_void_p(_ptr(src)), _sz3(src), C.c_void_p(_ptr(dst)), _sz3(dst),
-                                         C.c_void_p(stream or 0)), ctx, "tw_warp_affine_device")
+                                         C.c_void_p(_stream_arg(stream, src, dst))), ctx, "tw_warp_affine_device")
 
 
 def imgwarp_smallmemory_image(ctx: Context, ql_marker_tar, ql_marker_sub, szBlock_x: int, szBlock_y: int,

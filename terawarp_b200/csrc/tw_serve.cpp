@@ -231,18 +231,16 @@ tw_status batch_round(tw_server *s, std::vector<JobRec *> &ready)
                 rj.push_back(affine_job(j->d_src, sp.src_sz, j->d_dst, sp.dst_sz, sp.M, sp.dtype, sp.interp));
         }
         TW_TRY(run_jobs(ctx, rj.data(), (int)rj.size(), s->batch));
-        cudaEvent_t done;
-        TW_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-        TW_CUDA_TRY(cudaEventRecord(done, s->batch));
+        // each job's stream continues after its own resample-end event, so a
+        // job's completion is never stamped before the end of its resample
+        for (JobRec *j : kv.second) TW_CUDA_TRY(cudaEventRecord(j->ev[JobRec::kRs1], s->batch));
         for (JobRec *j : kv.second) {
-            TW_CUDA_TRY(cudaEventRecord(j->ev[JobRec::kRs1], s->batch));
-            TW_CUDA_TRY(cudaStreamWaitEvent(j->st, done, 0));
+            TW_CUDA_TRY(cudaStreamWaitEvent(j->st, j->ev[JobRec::kRs1], 0));
             if (j->own_dst)
                 TW_CUDA_TRY(cudaMemcpyAsync(j->spec.dst, j->d_dst, j->dst_b, cudaMemcpyDeviceToHost, j->st));
             TW_CUDA_TRY(cudaEventRecord(j->ev[JobRec::kDone], j->st));
             j->state = kComputing;
         }
-        cudaEventDestroy(done);  // destruction is deferred until the event completes
     }
     return TW_OK;
 }

@@ -57,7 +57,7 @@ def _warp_both(ctx, vol, sub, tar, g):
 def test_staged_equals_gathered_bit_for_bit(ctx, g, dtype):
     shape = (96, 160, 320)  # z, y, x: a few units per axis, partial units at the far x / y / z ends
     case = synth.large_tps_case(77 + g, "cuda", shape_zyx=shape, n=200, g=g, n_blobs=400, n_fibres=40)
-    vol = case.vol if dtype == "u16" else (case.vol >> 4).to(torch.uint8)
+    vol = case.vol if dtype == "u16" else (case.vol.to(torch.int32) >> 4).to(torch.uint8)
     (staged, gathered), _ = _warp_both(ctx, vol, case.marker_sub, case.marker_tar, g)
     assert torch.equal(staged, gathered)
 
