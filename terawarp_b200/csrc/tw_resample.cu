@@ -9,15 +9,16 @@
 // TPS units (reference: q_dfblcokinterp_bspline + q_imgblockwarp,
 // q_imgwarp_tps_quicksmallmemory.cpp:85-203, and chazhi.cu:226-338, which
 // does a dense 64x64x3 matvec per 4^3 cell and gathers every voxel from
-// global memory): a column of 64 x 16 output voxels walks down its planes.
-// The cubic B-spline is evaluated separably: per cell layer the 4 x (CY+3) x
-// (CX+3) nodes are staged in shared memory as node' = DF + node position -
-// frame origin (the B-spline reproduces linear functions, so the spline of
-// node' is the sample position q itself), contracted along y once per layer
-// (R), along z once per output plane (Q), and along x per voxel (12 FMA) --
-// ~14 FMA per voxel instead of 192.  The column's source footprint is staged
-// in shared memory by TMA, plane by plane, so that the eight taps of every
-// voxel are shared-memory loads (see "TPS units" below).
+// global memory): a column of 64 x 16 output voxels walks down its planes,
+// one warp per output row.  The cubic B-spline is evaluated separably: per
+// cell layer a row warp contracts its row's nodes, taken as node' = DF +
+// node position - frame origin (the B-spline reproduces linear functions, so
+// the spline of node' is the sample position q itself), along y and then
+// along x into four position pairs per lane; per output plane the positions
+// are their z contraction -- 12 FFMA2 per voxel pair instead of 192 FMA per
+// voxel.  A copy warp stages the column's source footprint in shared memory
+// by TMA, plane by plane, so that the eight taps of every voxel are
+// shared-memory loads (see "TPS units" below).
 //
 // Affine bricks are 256 x 8 x 8 output voxels gathered from global memory.
 //
@@ -209,38 +210,6 @@ __device__ __forceinline__ int find_job(const RJob *jobs, int njobs, int64_t b)
     return lo;
 }
 
-// Block-wide min/max reduction of 3 components (6 floats), result broadcast.
-__device__ __forceinline__ void block_minmax(float (&mn)[3], float (&mx)[3], float *red)
-{
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
-            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
-        }
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            red[warp * 6 + a] = mn[a];
-            red[warp * 6 + 3 + a] = mx[a];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float m0 = red[a], m1 = red[3 + a];
-        for (int w = 1; w < kThreads / 32; ++w) {
-            m0 = fminf(m0, red[w * 6 + a]);
-            m1 = fmaxf(m1, red[w * 6 + 3 + a]);
-        }
-        mn[a] = m0;
-        mx[a] = m1;
-    }
-}
-
 // Is every brick-relative sample position in [lo, hi] strictly inside both
 // the subject volume and the source buffer, and are all byte offsets
 // representable in 32 bits?
@@ -354,23 +323,6 @@ __device__ __forceinline__ PairW make_pairw(const float4 (&wx)[2])
         p.wz[a] = f2(a0[a], a1[a]);
     }
     return p;
-}
-
-// Sample positions of a TPS voxel pair from its 4 x-taps: (qx, qy) of voxel
-// 0 and of voxel 1, and (qz0, qz1).
-__device__ __forceinline__ void pair_positions(const float4 n[4], const PairW &pw, float2 &p0, float2 &p1, float2 &pz2)
-{
-    p0 = make_float2(0.f, 0.f);
-    p1 = p0;
-    pz2 = p0;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const float2 xy = f2(n[a].x, n[a].y);
-        const float2 zz = f2(n[a].z, n[a].w);  // Q stores (x, y, z, z)
-        p0 = fma2(pw.w0[a], xy, p0);
-        p1 = fma2(pw.w1[a], xy, p1);
-        pz2 = fma2(pw.wz[a], zz, pz2);
-    }
 }
 
 // The four source rows a trilinear sample reads, (dy, dz) = (r & 1, r >> 1),
@@ -593,60 +545,79 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 
 // ------------------------------------------------------------- TPS units
 //
-// A TPS work unit is a column of 64 x 16 output voxels (x, y) over a run of
-// output planes: part of one control-cell layer (small jobs) or several
-// whole layers.  The unit walks its planes in order.  Each cell layer is
-// evaluated in its own frame -- origin at the column's corner on the layer's
-// first plane -- so a voxel's position and value do not depend on how the
-// volume is cut into units or how units are batched.  Lane l of warp w owns
-// the voxel pair (2l, 2l+1) of rows w and w+8: a warp covers one whole row,
-// so its taps for one source row are 64 consecutive-ish voxels.
+// A TPS work unit is a column of 64 x 16 output voxels (x, y) walking down a
+// run of output planes: part of one control-cell layer (small jobs) or
+// several whole layers.  Each cell layer is evaluated in its own frame --
+// origin at the column's corner on the layer's first plane -- so a voxel's
+// position and value do not depend on how the volume is cut into units or
+// how units are batched.
+//
+// A CTA is 16 row warps and one copy warp.  Row warp w owns output row w of
+// the unit; lane l owns the voxel pair (2l, 2l+1), so a warp covers one whole
+// 64-voxel row.  Per cell layer a row warp contracts the 4 x 4 x (64/G + 3)
+// nodes of its row along y (into warp-private shared memory), then every
+// lane contracts them along x for its voxel pair: four (one per node layer
+// along z) position pairs P_c kept in registers.  Per output plane the
+// positions are sum_c wz_c P_c (12 FFMA2 per pair); no node data is touched
+// and no barrier is taken.
 //
 // Staged walks.  The column's source footprint over a walk -- the convex
-// hull of its B-spline nodes' displacements (weights >= 0, sum 1) plus the
-// +1 tap -- is a box of at most kBoxW x kHMax elements per source plane and
-// a window of planes that slides down one plane per output plane.  The box's
-// rows are copied into a ring of plane slots in shared memory by TMA
-// (cp.async.bulk.tensor, one row per copy from this GPU's own memory,
-// completion counted on one mbarrier per slot), kAhead planes ahead of the
-// plane being sampled, and every tap becomes a shared-memory load.  Slot 0
-// also has a copy one slot past the end, so the z+1 tap of any plane is at a
-// fixed offset.  The slots' row pitch is 128 elements: a step of a row or a
-// plane then moves an address by a multiple of 32 banks, so the loads of a
-// warp's 64 voxels hit 32 distinct banks whichever rows and planes the lanes
-// read.  A walk whose box or window does not fit, a nearest-neighbour job,
-// or a source buffer TMA cannot describe gathers from global memory instead,
-// with the same positions and the same trilinear arithmetic (trilerp2).
+// hull of its nodes' displacements (B-spline weights are >= 0 and sum to 1)
+// plus the +1 tap -- is a box of at most kBoxW x kHMax elements per source
+// plane and a window of W planes that slides down one plane per output
+// plane.  The copy warp plans each walk, publishes the plan, and copies the
+// box's rows of every source plane the walk reads, in order, into a ring of
+// kRing plane slots by TMA (cp.async.bulk.tensor, one row per copy, from this
+// GPU's own memory; no multicast).  Each slot has a "full" mbarrier
+// (transaction count of the copies) and an "empty" mbarrier (one arrival per
+// row warp once no later plane of that warp reads the slot): the copy warp
+// refills a slot as soon as every row warp has released it, so copies run
+// up to kRing - W planes ahead of the slowest row warp and row warps never
+// wait for one another.  Slot 0 is copied a second time past the last slot,
+// so the z+1 tap of any plane is at a fixed offset.  The slots' row pitch is
+// 128 elements: a row or plane step moves an address by a multiple of 32
+// banks, so a warp's loads hit distinct banks whichever rows and planes its
+// lanes read.  A walk whose box or window does not fit, a nearest-neighbour
+// job, or a source buffer TMA cannot describe gathers from global memory
+// instead, with the same positions and the same trilinear arithmetic
+// (trilerp2).
 
-constexpr int kTBX = 64;               // unit width (x): 32 lanes x 2 voxels
-constexpr int kTBY = 16;               // unit height (y)
-constexpr int kTRows = kTBY / kTY;     // rows per warp
-constexpr int kBoxW = kStageBoxW;      // TMA box: source elements per row copy
-constexpr int kRowP = 128;             // shared-memory row pitch (elements)
-constexpr int kHMax = 28;              // staged rows per plane
-constexpr int kAhead = 2;              // planes copied ahead of the plane being sampled
-// a staged plane that has not landed after this long is an error (the wait
-// gives up, the kernel reports kKernErrTimeout and returns)
+constexpr int kTBX = 64;                     // unit width (x): 32 lanes x 2 voxels
+constexpr int kTBY = 16;                     // unit height (y): one row warp per row
+constexpr int kRowWarps = kTBY;
+constexpr int kTpsThreads = 32 * (kRowWarps + 1);  // + the copy warp
+constexpr int kBoxW = kStageBoxW;            // TMA box: source elements per row copy
+constexpr int kRowP = 128;                   // shared-memory row pitch (elements)
+constexpr int kHMax = 28;                    // staged rows per plane
+constexpr int kRing = 24;                    // plane slots (plus the mirror of slot 0)
+constexpr int kMinAhead = 2;                 // slots a walk's window leaves for copies in flight
+// a wait on a copy or on another warp that has not ended after this long is
+// an error (the kernel reports kKernErrTimeout and returns)
 constexpr unsigned long long kStageWaitNs = 2000000000ull;
+
+// A walk's staging plan, written by the copy warp, read by the row warps.
+struct alignas(16) Plan {
+    int staged;    // 1: the walk's source footprint is staged
+    int a, b;      // output plane z reads source planes [z + a, z + b]
+    int rx0, ry0;  // buffer column / row of the staged box's first element
+    int rows;      // staged rows per plane
+    int DX, DY;    // box column / row of frame x = 0 / y = 0
+    int nplanes;   // source planes staged for the walk
+    int pad[3];
+};
 
 template <typename T, int G>
 struct TGeom {
-    static constexpr int CX = kTBX / G;               // cells along x (G <= 64)
-    static constexpr int CY = G < kTBY ? kTBY / G : 1; // cell rows a unit's 16 rows touch
-    static constexpr int NX = CX + 3;
-    static constexpr int NY = CY + 3;
-    static constexpr int ND = 4 * NY * NX;            // staged nodes of one layer
-    static constexpr int NR = kTBY * 4 * NX;          // y-contracted
-    static constexpr int NQ = 2 * kTBY * NX;          // z-contracted, double-buffered
-    static constexpr int UNION = ND > NQ ? ND : NQ;
-    static constexpr int R = G == 4 ? 10 : 12;        // ring slots (plus the mirror of slot 0)
+    static constexpr int NX = kTBX / G + 3;       // node columns of a unit (G <= 64)
+    static constexpr int NRW = 4 * NX;            // y-contracted nodes of one row and layer
     static constexpr int ES = (int)sizeof(T);
     static constexpr int ROW_B = kRowP * ES;
     static constexpr int PLANE_B = kHMax * ROW_B;
-    static constexpr int RING_B = (R + 1) * PLANE_B;
-    static constexpr int MBAR_B = 8 * 16;
-    static constexpr size_t smem_bytes = 128 + (size_t)RING_B + MBAR_B + sizeof(float4) * (size_t)(UNION + NR + G);
-    static_assert(R <= 16, "one mbarrier per slot, 16 at most");
+    static constexpr int RING_B = (kRing + 1) * PLANE_B;
+    static constexpr int NBAR = 2 * kRing + 4;    // full[kRing], empty[kRing], plan full[2], plan empty[2]
+    static constexpr size_t smem_bytes =
+        128 + (size_t)RING_B + 8 * NBAR + 2 * sizeof(Plan) + sizeof(float4) * (size_t)(G + kRowWarps * NRW);
+    static_assert((8 * NBAR) % 16 == 0, "the weight table is float4-aligned");
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
@@ -666,6 +637,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t a)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
 {
     uint32_t ok;
@@ -680,19 +656,20 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
 }
 
 // Waits for the phase of parity `parity` of the mbarrier at `a`; gives up
-// (false) after kStageWaitNs.
-__device__ __noinline__ bool mbar_wait_slow(uint32_t a, uint32_t parity)
+// (false) after kStageWaitNs, or early once another warp has given up
+// (*abort set) unless `drain`.
+__device__ __noinline__ bool mbar_wait_slow(uint32_t a, uint32_t parity, const volatile int *abort, bool drain)
 {
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned i = 1;; ++i) {
         if (mbar_try(a, parity)) return true;
-        if ((i & 255u) == 0 && globaltimer_ns() - t0 > kStageWaitNs) return false;
+        if ((i & 63u) == 0 && ((!drain && *abort) || globaltimer_ns() - t0 > kStageWaitNs)) return false;
     }
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, const volatile int *abort)
 {
-    return mbar_try(a, parity) || mbar_wait_slow(a, parity);
+    return mbar_try(a, parity) || mbar_wait_slow(a, parity, abort, false);
 }
 
 // One row of a staged plane: kBoxW elements at tensor coordinates (x, y, z)
@@ -707,80 +684,321 @@ __device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, in
         : "memory");
 }
 
-__device__ __forceinline__ int pmod(int64_t p, int r)
-{
-    const int64_t m = p % r;
-    return (int)(m < 0 ? m + r : m);
-}
-
 // Shared memory of a TPS CTA.
-template <typename T, int G>
 struct TSmem {
     unsigned char *base;  // 128-byte aligned start of the ring
     uint32_t sring;       // shared-window address of slot 0
-    uint32_t smbar;       // shared-window address of slot 0's mbarrier (8 bytes each)
-    float4 *Nd, *Qb, *R, *W;
+    uint32_t sfull;       // shared-window address of full[0] (8 bytes each); empty[s] = full[s] + 8 kRing
+    uint32_t splan;       // plan full[0..1], then plan empty[0..1]
+    Plan *plans;          // two plan slots
+    float4 *W;            // B-spline weights at t = i / G
+    float4 *Rw;           // per row warp: y-contracted nodes of its row
+    int *abort;           // set by a warp that gave up waiting
 };
 
-// State of a staged walk; every thread holds the same values.
-struct Stage {
-    int a, b;             // output plane z reads source planes [z + a, z + b]
-    int rx0, ry0, rows;   // staged box: buffer column and row of its first element, rows per plane
-    int DX, DY;           // box column / row of frame x = 0 / y = 0
-    int64_t issued;       // last plane copied (buffer z)
-    int64_t waited;       // last plane this thread waited for (buffer z)
-    int64_t last;         // last plane the walk reads (buffer z)
-    uint32_t kxy;         // offset (from base) of frame x = y = 0 in slot 0, magic-float bias folded in
-    uint32_t omax;        // largest offset whose 8 taps all stay inside the ring
+// Job and unit of flattened unit index u.
+struct Walk {
+    int j;
+    int64_t Ox, Oy, z0, z1;
 };
 
-// Copies staged plane p (buffer z) into its slot; executed by warp 0.
+__device__ __forceinline__ Walk walk_of(const RJob *jobs, int njobs, int64_t u)
+{
+    Walk w;
+    w.j = find_job(jobs, njobs, u);
+    const RJob &J = jobs[w.j];
+    const int64_t lu = u - J.brick_begin;
+    const int64_t bx = lu % J.bricks[0], t = lu / J.bricks[0];
+    const int64_t by = t % J.bricks[1], bz = t / J.bricks[1];
+    w.Ox = J.out_o[0] + bx * kTBX;
+    w.Oy = J.out_o[1] + by * kTBY;
+    w.z0 = J.out_o[2] + bz * J.zs;
+    w.z1 = min(w.z0 + (int64_t)J.zs, J.out_o[2] + J.out_n[2]);
+    return w;
+}
+
+// Warp-wide min / max of 3 components.
+__device__ __forceinline__ void warp_minmax(float (&mn)[3], float (&mx)[3])
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+        }
+}
+
+// Plans walk w (copy warp): the hull of the DF over the walk's node support
+// gives the staged box and the plane window.  staged = 0 when they do not
+// fit.  Every lane returns the same plan.
 template <typename T, int G>
-__device__ __forceinline__ void stage_issue(const RJob &J, const TSmem<T, G> &S, const Stage &st, int64_t p, int lane)
+__device__ Plan plan_walk(const RJob &J, const Walk &w)
+{
+    constexpr int NX = TGeom<T, G>::NX;
+    constexpr int NY = (G < kTBY ? kTBY / G : 1) + 3;
+    Plan P = {};
+    const int lane = threadIdx.x & 31;
+    const int64_t cx0 = w.Ox / G, cy0 = w.Oy / G, cz0 = w.z0 / G;
+    const int nzn = (int)((w.z1 - 1) / G - cz0) + 4;
+    const int tot = NX * NY * nzn;
+    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    for (int i = lane; i < tot; i += 32) {
+        const int nx = i % NX, t = i / NX;
+        const int ny = t % NY, nz = t / NY;
+        const int64_t gx = min(cx0 + nx, J.gsz[0] - 1), gy = min(cy0 + ny, J.gsz[1] - 1);
+        const int64_t gz = min(cz0 + nz, J.gsz[2] - 1);
+        const float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
+        if (isfinite(d.x) && isfinite(d.y) && isfinite(d.z)) {
+            mn[0] = fminf(mn[0], d.x); mn[1] = fminf(mn[1], d.y); mn[2] = fminf(mn[2], d.z);
+            mx[0] = fmaxf(mx[0], d.x); mx[1] = fmaxf(mx[1], d.y); mx[2] = fmaxf(mx[2], d.z);
+        } else {
+            mn[0] = mn[1] = mn[2] = -3.4e38f;
+            mx[0] = mx[1] = mx[2] = 3.4e38f;
+        }
+    }
+    warp_minmax(mn, mx);
+    for (int a = 0; a < 3; ++a)
+        if (!(mn[a] > -1.0e6f && mx[a] < 1.0e6f)) return P;
+    // taps of the walk, frame coordinates: x in [fx0, 63 + fx1 + 1], y in
+    // [fy0, 15 + fy1 + 1], z in [z + fz0, z + fz1 + 1] for output plane z (a
+    // margin of 1/64 covers the FP32 rounding of the spline)
+    const float e = 1.0f / 64.0f;
+    const int fx0 = (int)floorf(mn[0] - e), fx1 = (int)floorf(mx[0] + e);
+    const int fy0 = (int)floorf(mn[1] - e), fy1 = (int)floorf(mx[1] + e);
+    const int fz0 = (int)floorf(mn[2] - e), fz1 = (int)floorf(mx[2] + e);
+    // the box's first column, in source-buffer coordinates, on a 16-byte boundary
+    constexpr int A = 16 / (int)sizeof(T);
+    const int64_t xlo = w.Ox - J.src_o[0] + fx0;
+    const int64_t xhi = w.Ox - J.src_o[0] + kTBX + fx1;
+    const int64_t rx0 = xlo >= 0 ? (xlo / A) * A : -(((-xlo) + A - 1) / A) * A;
+    if (xhi - rx0 + 1 > kBoxW) return P;
+    const int rows = kTBY + fy1 - fy0 + 1;
+    if (rows > kHMax) return P;
+    const int a = fz0, b = fz1 + 1;
+    if (b - a + 1 + kMinAhead > kRing) return P;
+    const int64_t ry0 = w.Oy - J.src_o[1] + fy0;
+    const int64_t p0 = w.z0 + a - J.src_o[2], p1 = w.z1 - 1 + b - J.src_o[2];
+    const int64_t lim = (int64_t)1 << 30;  // TMA coordinates are int32
+    if (rx0 < -lim || rx0 > lim || ry0 < -lim || ry0 + rows > lim || p0 < -lim || p1 > lim) return P;
+    P.staged = 1;
+    P.a = a;
+    P.b = b;
+    P.rx0 = (int)rx0;
+    P.ry0 = (int)ry0;
+    P.rows = rows;
+    P.DX = (int)(w.Ox - J.src_o[0] - rx0);
+    P.DY = -fy0;
+    P.nplanes = (int)(w.z1 - w.z0) + b - a;
+    return P;
+}
+
+// The copy warp: plans every walk of the CTA, publishes each plan, and
+// copies each staged walk's source planes into the ring, in order.  Returns
+// false if a wait gave up.
+template <typename T, int G, int INTERP>
+__device__ bool tps_copier(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
 {
     using Gm = TGeom<T, G>;
-    const int s = pmod(p, Gm::R);
-    const uint32_t mb = S.smbar + 8u * (uint32_t)s;
-    const uint32_t bytes = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)st.rows * (s == 0 ? 2u : 1u);
-    if (lane == 0) mbar_expect_tx(mb, bytes);
+    const int lane = threadIdx.x & 31;
+    uint32_t seq = 0;  // source planes copied so far (ring sequence number)
+    uint32_t slot = 0;
+    int last_job = -1;
+    int64_t u = blockIdx.x;
+    if (u >= total) return true;
+    Walk w = walk_of(jobs, njobs, u);
+    auto plan_of = [&](const Walk &wk) -> Plan {
+        const RJob &J = jobs[wk.j];
+        if (INTERP != 0 || !J.tma_ok) return Plan{};
+        if (wk.j != last_job)  // the descriptor was written by a copy
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
+        last_job = wk.j;
+        return plan_walk<T, G>(J, wk);
+    };
+    Plan nxt = plan_of(w);
+    bool ok = true;
+    for (uint32_t k = 0;; ++k) {
+        const Plan P = nxt;
+        const RJob &J = jobs[w.j];
+        // publish the plan (its slot is free once every row warp has read
+        // the plan two walks back)
+        const uint32_t q = k & 1u;
+        if (k >= 2 && !mbar_wait(S.splan + 16u + 8u * q, ((k >> 1) - 1u) & 1u, S.abort)) { ok = false; break; }
+        if (lane == 0) S.plans[q] = P;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(S.splan + 8u * q);
+        const int64_t un = u + gridDim.x;
+        const bool more = un < total;
+        Walk wn = w;
+        if (more) wn = walk_of(jobs, njobs, un);
+        bool planned = !more;
+        // copy the walk's planes; the next walk is planned once this walk's
+        // first window is on its way
+        const int64_t pfirst = w.z0 + P.a - J.src_o[2];
+        const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)P.rows;
+        for (int i = 0; i < P.nplanes; ++i) {
+            if (!planned && i == P.b - P.a + 1) {
+                nxt = plan_of(wn);
+                planned = true;
+            }
+            const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
+            if (seq >= (uint32_t)kRing && !mbar_wait(empty, (seq / kRing - 1u) & 1u, S.abort)) { ok = false; break; }
+            if (lane == 0) mbar_expect_tx(full, slot == 0 ? 2u * bytes1 : bytes1);
+            __syncwarp();
+            if (lane < P.rows) {
+                // the row warps' reads of the slot's previous plane happen
+                // before their release of it; order them before the
+                // asynchronous write
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B + (uint32_t)(lane * Gm::ROW_B);
+                const int pz = (int)(pfirst + i);
+                tma_row(d, &J.tmap, P.rx0, P.ry0 + lane, pz, full);
+                if (slot == 0) tma_row(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, P.rx0, P.ry0 + lane, pz, full);
+            }
+            ++seq;
+            slot = slot + 1 == (uint32_t)kRing ? 0u : slot + 1;
+        }
+        if (!ok) break;
+        if (!more) break;
+        if (!planned) nxt = plan_of(wn);
+        u = un;
+        w = wn;
+    }
+    // every copy issued lands before the CTA exits (bounded waits)
+    const uint32_t n0 = seq > (uint32_t)kRing ? seq - kRing : 0u;
+    for (uint32_t n = n0; n < seq; ++n)
+        if (!mbar_try(S.sfull + 8u * (n % kRing), (n / kRing) & 1u))
+            mbar_wait_slow(S.sfull + 8u * (n % kRing), (n / kRing) & 1u, S.abort, true);
+    return ok;
+}
+
+// The row warps' state of one cell layer (uniform across the warp except
+// the position pairs).
+struct RowLayer {
+    float2 P[4][3];   // per node layer c: (x, y) of voxel 0, (x, y) of voxel 1, (z0, z1)
+    Frame frame;
+    Clamp cw;
+    float zlo, zhi;   // a plane at frame z pz is unchecked in z when zlo <= pz < zhi
+    bool row_fast;    // the row is unchecked in x and y
+};
+
+// Layer setup of row warp `y` of the unit at (Ox, Oy), layer frame origin
+// Oz: y-contraction of the row's nodes into Rw, x-contraction into the
+// lane's position pairs, and the row's sample hull.
+template <typename T, int G>
+__device__ __forceinline__ void row_layer(const RJob &J, int64_t Ox, int64_t Oy, int64_t Oz, int zoff, int zn, int y,
+                                          int xe, const float4 *W, float4 *Rw, const float4 (&wx)[2], RowLayer &L)
+{
+    using Gm = TGeom<T, G>;
+    const int lane = threadIdx.x & 31;
+    const int64_t O[3] = {Ox, Oy, Oz};
+    const int64_t c0[3] = {Ox / G, Oy / G, Oz / G};
+    const int yy = (int)(Oy - c0[1] * G) + y;
+    const int cyb = yy / G;
+    const float4 wy = W[yy % G];
+    __syncwarp();  // every lane is done with the previous layer's Rw
+    // R[c][nx] = sum_b wy_b node'[c][cyb + b][nx], node' = DF + node position - O
+    for (int i = lane; i < Gm::NRW; i += 32) {
+        const int c = i / Gm::NX, nx = i % Gm::NX;
+        const int64_t gx = min(c0[0] + nx, J.gsz[0] - 1), gz = min(c0[2] + c, J.gsz[2] - 1);
+        // node g sits at (g-1)*G; relative to O that is exact in float
+        const float ox = (float)((gx - 1) * G - O[0]), oz = (float)((gz - 1) * G - O[2]);
+        float4 v[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int64_t gy = min(c0[1] + cyb + b, J.gsz[1] - 1);
+            const float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
+            v[b] = make_float4(d.x + ox, d.y + (float)((gy - 1) * G - O[1]), d.z + oz, 0.f);
+        }
+        float4 r;
+        r.x = fmaf(wy.x, v[0].x, fmaf(wy.y, v[1].x, fmaf(wy.z, v[2].x, wy.w * v[3].x)));
+        r.y = fmaf(wy.x, v[0].y, fmaf(wy.y, v[1].y, fmaf(wy.z, v[2].y, wy.w * v[3].y)));
+        r.z = fmaf(wy.x, v[0].z, fmaf(wy.y, v[1].z, fmaf(wy.z, v[2].z, wy.w * v[3].z)));
+        r.w = 0.f;
+        Rw[i] = r;
+    }
     __syncwarp();
-    if (lane < st.rows) {
-        // the slot's previous plane was read by every thread before the
-        // barrier that precedes this call; order those generic-proxy reads
-        // before the asynchronous write
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const uint32_t d = S.sring + (uint32_t)(s * Gm::PLANE_B + lane * Gm::ROW_B);
-        tma_row(d, &J.tmap, st.rx0, st.ry0 + lane, (int)p, mb);
-        if (s == 0) tma_row(d + (uint32_t)(Gm::R * Gm::PLANE_B), &J.tmap, st.rx0, st.ry0 + lane, (int)p, mb);
+    // x-contraction for the lane's voxel pair (2 lane, 2 lane + 1: one cell)
+    const int xn = (2 * lane) / G;
+    float dmn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, dmx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    bool fin = true;
+    const float x0 = (float)(2 * lane), fy = (float)y;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float2 p0 = f2(0.f, 0.f), p1 = p0, pz = p0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const float4 n = Rw[c * Gm::NX + xn + a];
+            const float w0 = (&wx[0].x)[a], w1 = (&wx[1].x)[a];
+            p0 = fma2(f2(w0, w0), f2(n.x, n.y), p0);
+            p1 = fma2(f2(w1, w1), f2(n.x, n.y), p1);
+            pz = fma2(f2(w0, w1), f2(n.z, n.z), pz);
+        }
+        L.P[c][0] = p0;
+        L.P[c][1] = p1;
+        L.P[c][2] = pz;
+        // displacement part (the spline of the node positions is the voxel
+        // position; node layer c sits at frame z (c - 1) G)
+        const float zc = (float)((c - 1) * G);
+        const float d[6] = {p0.x - x0, p1.x - (x0 + 1.f), p0.y - fy, p1.y - fy, pz.x - zc, pz.y - zc};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            fin = fin && isfinite(d[k]);
+            dmn[k >> 1] = fminf(dmn[k >> 1], d[k]);
+            dmx[k >> 1] = fmaxf(dmx[k >> 1], d[k]);
+        }
     }
+    warp_minmax(dmn, dmx);
+    if (!__all_sync(0xffffffffu, fin))
+        for (int a = 0; a < 3; ++a) {
+            dmn[a] = -3.4e38f;
+            dmx[a] = 3.4e38f;
+        }
+    // sample hull of the row over the layer's planes (frame coordinates)
+    const float plo[3] = {0.f, fy, (float)zoff};
+    const float phi[3] = {(float)(kTBX - 1), fy, (float)(zoff + zn - 1)};
+    float mn[3], mx[3];
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = dmn[a] <= -3.0e38f ? -3.4e38f : plo[a] + dmn[a];
+        mx[a] = dmx[a] >= 3.0e38f ? 3.4e38f : phi[a] + dmx[a];
+    }
+    L.frame = make_frame(J, O);
+    const bool span_ok = offsets_fit_32(J, mn, mx);
+    L.cw = make_clamp(J, L.frame, mn, mx);
+    // unchecked-path bounds per axis: every tap of a sample q with
+    // lb <= q < hb lies inside the volume and the source buffer
+    float lb[3], hb[3];
+    for (int a = 0; a < 3; ++a) {
+        lb[a] = fmaxf(L.frame.lo[a], (float)L.frame.bl[a]) + 1.0f / 64.0f;
+        hb[a] = fminf(L.frame.hi[a], (float)L.frame.bh[a]) - 1.0f / 64.0f;
+    }
+    L.row_fast = span_ok && L.cw.span32 && (kTBX <= xe) && mn[0] >= lb[0] && mx[0] < hb[0] && mn[1] >= lb[1] &&
+                 mx[1] < hb[1];
+    L.zlo = lb[2] - dmn[2];
+    L.zhi = hb[2] - dmx[2];
 }
 
-// Waits for every plane up to `upto` (buffer z); false if a wait gave up.
-template <typename T, int G>
-__device__ __forceinline__ bool stage_wait(const TSmem<T, G> &S, Stage &st, uint32_t &parity, int64_t upto)
+// Positions of the lane's voxel pair on a plane with z weights wz.
+__device__ __forceinline__ void plane_positions(const RowLayer &L, float4 wz, float2 &p0, float2 &p1, float2 &pz)
 {
-    using Gm = TGeom<T, G>;
-    while (st.waited < upto) {
-        const int64_t p = st.waited + 1;
-        const int s = pmod(p, Gm::R);
-        if (!mbar_wait(S.smbar + 8u * (uint32_t)s, (parity >> s) & 1u)) return false;
-        parity ^= 1u << s;
-        st.waited = p;
-    }
-    return true;
+    const float2 w0 = f2(wz.x, wz.x), w1 = f2(wz.y, wz.y), w2 = f2(wz.z, wz.z), w3 = f2(wz.w, wz.w);
+    p0 = fma2(w0, L.P[0][0], fma2(w1, L.P[1][0], fma2(w2, L.P[2][0], fma2(w3, L.P[3][0], f2(0.f, 0.f)))));
+    p1 = fma2(w0, L.P[0][1], fma2(w1, L.P[1][1], fma2(w2, L.P[2][1], fma2(w3, L.P[3][1], f2(0.f, 0.f)))));
+    pz = fma2(w0, L.P[0][2], fma2(w1, L.P[1][2], fma2(w2, L.P[2][2], fma2(w3, L.P[3][2], f2(0.f, 0.f)))));
 }
 
-// Offset (from base) of the (x, y, z) = floor tap of a staged sample, from the
-// magic-floor bit patterns; clamped so that all 8 taps stay in the ring.
-template <typename T, int G>
-__device__ __forceinline__ uint32_t staged_off(const Stage &st, uint32_t cz, float mx, float my, float mz)
+// Offset (from the ring base) of the (x, y, z) = floor tap of a staged
+// sample, from the magic-floor bit patterns; cz maps a tap plane to its
+// slot (the ring wrap is one unsigned min); clamped so that all 8 taps stay
+// in the ring.
+template <typename T>
+__device__ __forceinline__ uint32_t staged_off(uint32_t kxy, uint32_t omax, uint32_t cz, float mx, float my, float mz)
 {
-    using Gm = TGeom<T, G>;
-    const uint32_t t = __float_as_uint(mz) + cz;  // slot + (0 or R) for the planes of the window
-    const uint32_t slot = min(t, t - (uint32_t)Gm::R);
-    const uint32_t o = slot * (uint32_t)Gm::PLANE_B + __float_as_uint(my) * (uint32_t)Gm::ROW_B +
-                       __float_as_uint(mx) * (uint32_t)Gm::ES + st.kxy;
-    return min(o, st.omax);
+    constexpr uint32_t ROW_B = kRowP * sizeof(T), PLANE_B = kHMax * ROW_B;
+    const uint32_t t = __float_as_uint(mz) + cz;  // slot, or slot + kRing past the wrap
+    const uint32_t slot = min(t, t - (uint32_t)kRing);
+    const uint32_t o = slot * PLANE_B + __float_as_uint(my) * ROW_B + __float_as_uint(mx) * (uint32_t)sizeof(T) + kxy;
+    return min(o, omax);
 }
 
 // Magic float 2^23 + v of the staged voxel at offset o.
@@ -795,12 +1013,12 @@ __device__ __forceinline__ float smag(const unsigned char *sm, uint32_t o)
 // into the staged window (wl, wh: frame coordinates) so that no tap of an
 // invalid sample leaves it; for a valid sample the clamp changes nothing (the
 // window holds the whole footprint), so both variants give the same bits.
-template <typename T, int G, bool ROUND, bool CHECKED>
-__device__ __forceinline__ uint32_t pair_staged(const unsigned char *sm, const Stage &st, uint32_t cz, float2 p0,
-                                                float2 p1, float2 pz2, const Frame &f, const float (&wl)[3],
+template <typename T, bool CHECKED>
+__device__ __forceinline__ uint32_t pair_staged(const unsigned char *sm, uint32_t kxy, uint32_t omax, uint32_t cz,
+                                                float2 p0, float2 p1, float2 pz2, const Frame &f, const float (&wl)[3],
                                                 const float (&wh)[3], int nvalid)
 {
-    using Gm = TGeom<T, G>;
+    constexpr uint32_t ES = sizeof(T), ROW_B = kRowP * ES, PLANE_B = kHMax * ROW_B;
     const float2 MM = f2(kMagic, kMagic);
     float2 m0, m1, mz, f0, f1, fz;
     bool ok0 = true, ok1 = true;
@@ -828,410 +1046,178 @@ __device__ __forceinline__ uint32_t pair_staged(const unsigned char *sm, const S
         f1 = sub2(p1, sub2(m1, MM));
         fz = sub2(pz2, sub2(mz, MM));
     }
-    const uint32_t o0 = staged_off<T, G>(st, cz, m0.x, m0.y, mz.x);
-    const uint32_t o1 = staged_off<T, G>(st, cz, m1.x, m1.y, mz.y);
-    constexpr uint32_t rofs[4] = {0u, (uint32_t)Gm::ROW_B, (uint32_t)Gm::PLANE_B, (uint32_t)(Gm::PLANE_B + Gm::ROW_B)};
+    const uint32_t o0 = staged_off<T>(kxy, omax, cz, m0.x, m0.y, mz.x);
+    const uint32_t o1 = staged_off<T>(kxy, omax, cz, m1.x, m1.y, mz.y);
+    constexpr uint32_t rofs[4] = {0u, ROW_B, PLANE_B, PLANE_B + ROW_B};
     float2 lo[4], hi[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         lo[r] = f2(smag<T>(sm, o0 + rofs[r]), smag<T>(sm, o1 + rofs[r]));
-        hi[r] = f2(smag<T>(sm, o0 + rofs[r] + Gm::ES), smag<T>(sm, o1 + rofs[r] + Gm::ES));
+        hi[r] = f2(smag<T>(sm, o0 + rofs[r] + ES), smag<T>(sm, o1 + rofs[r] + ES));
     }
-    const float2 t = out_pair<T, ROUND>(trilerp2(lo, hi, f2(f0.x, f1.x), f2(f0.y, f1.y), fz));
+    const float2 t = out_pair<T, true>(trilerp2(lo, hi, f2(f0.x, f1.x), f2(f0.y, f1.y), fz));
     if (CHECKED)  // a rejected voxel writes 0: the bits of 2^23 have zero low bits
         return pack_pair<T>(ok0 ? __float_as_uint(t.x) : 0x4B000000u, ok1 ? __float_as_uint(t.y) : 0x4B000000u);
     return pack_pair<T>(__float_as_uint(t.x), __float_as_uint(t.y));
 }
 
-// Everything a lane needs about its unit's current layer.
+// Global-memory sampling state of a row warp's layer (every path but the staged one).
 template <typename T>
-struct BrickCtx {
-    const T *base;      // source element at the frame origin (may lie outside the buffer)
-    int py32, pz32;     // source pitches as int (valid when the brick's offsets fit int32)
-    int64_t py, pz;     // source pitches
-    Frame frame;
-    Clamp cw;
+struct Gather {
+    const T *base;   // source element at the frame origin (may lie outside the buffer)
+    int py32, pz32;  // pitches as int (valid when the layer's offsets fit int32)
+    int64_t py, pz;
     Rows<T> rows;
-    PairW pw;           // packed x weights of the lane's voxel pair
-    float4 wx[2];       // scalar x weights (nearest-neighbour path)
-    bool pair_ok;       // a voxel pair can be stored as one 2-element word
-    int xe, ye;         // valid x / y extent of the unit's output region
 };
 
-// A voxel pair gathered from global memory (every path but the staged one).
-template <typename T, int G, int INTERP>
-__device__ __forceinline__ void tps_pair(const float4 (&n)[4], const BrickCtx<T> &B, int x, bool fast, T *drow)
+// A voxel pair gathered from global memory.
+template <typename T, int INTERP>
+__device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, const RowLayer &L, const Gather<T> &g,
+                                              bool fast, int nv, bool pair_ok, T *dp)
 {
     if constexpr (INTERP == 0) {
-        float2 p0, p1, pz2;
-        pair_positions(n, B.pw, p0, p1, pz2);
         uint32_t w;
-        if (fast) {
-            pair_fast2<T, true>(p0, p1, pz2, B.rows, w);
-            store_packed<T>(drow + x, w, B.pair_ok, 2);
-        } else {
-            const int nv = B.xe - x;
-            if (B.cw.clamped)
-                pair_clamped2<T, true>(p0, p1, pz2, B.rows, B.frame, B.cw.cl, B.cw.ch, nv, w);
-            else if (B.cw.span32)
-                pair_checked2<T, true, int>(p0, p1, pz2, B.base, B.py32, B.pz32, B.frame, B.cw.cl, B.cw.ch, nv, w);
-            else
-                pair_checked2<T, true, int64_t>(p0, p1, pz2, B.base, B.py, B.pz, B.frame, B.cw.cl, B.cw.ch, nv, w);
-            store_packed<T>(drow + x, w, B.pair_ok, nv);
-        }
+        if (fast)
+            pair_fast2<T, true>(p0, p1, pz2, g.rows, w);
+        else if (L.cw.clamped)
+            pair_clamped2<T, true>(p0, p1, pz2, g.rows, L.frame, L.cw.cl, L.cw.ch, nv, w);
+        else if (L.cw.span32)
+            pair_checked2<T, true, int>(p0, p1, pz2, g.base, g.py32, g.pz32, L.frame, L.cw.cl, L.cw.ch, nv, w);
+        else
+            pair_checked2<T, true, int64_t>(p0, p1, pz2, g.base, g.py, g.pz, L.frame, L.cw.cl, L.cw.ch, nv, w);
+        store_packed<T>(dp, w, pair_ok, fast ? 2 : nv);
     } else {
+        const float q[2][3] = {{p0.x, p0.y, pz2.x}, {p1.x, p1.y, pz2.y}};
         uint32_t outv[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const float4 w = B.wx[j];
-            const float qx = fmaf(w.x, n[0].x, fmaf(w.y, n[1].x, fmaf(w.z, n[2].x, w.w * n[3].x)));
-            const float qy = fmaf(w.x, n[0].y, fmaf(w.y, n[1].y, fmaf(w.z, n[2].y, w.w * n[3].y)));
-            const float qz = fmaf(w.x, n[0].z, fmaf(w.y, n[1].z, fmaf(w.z, n[2].z, w.w * n[3].z)));
             float v;
             if (fast) {
-                v = sample_fast<T, INTERP>(B.base, B.py32, B.pz32, qx, qy, qz);
-                outv[j] = INTERP == 1 ? (uint32_t)v : to_out<T, true>(v);
+                v = sample_fast<T, INTERP>(g.base, g.py32, g.pz32, q[j][0], q[j][1], q[j][2]);
+                outv[j] = (uint32_t)v;
             } else {
-                const bool ok =
-                    (x + j) < B.xe && sample_checked<T, INTERP>(B.base, B.py, B.pz, B.frame, qx, qy, qz, v);
-                outv[j] = ok ? (INTERP == 1 ? (uint32_t)v : to_out<T, true>(v)) : 0u;
+                const bool ok = j < nv && sample_checked<T, INTERP>(g.base, g.py, g.pz, L.frame, q[j][0], q[j][1],
+                                                                   q[j][2], v);
+                outv[j] = ok ? (uint32_t)v : 0u;
             }
         }
-        store_pair<T>(drow + x, outv[0], outv[1], B.pair_ok, fast ? 2 : B.xe - x);
+        store_pair<T>(dp, outv[0], outv[1], pair_ok, fast ? 2 : nv);
     }
 }
 
-// Planes [zf, zf + zn) of one cell layer of a unit (global output z), in the
-// layer's frame.  STAGED: the taps come from the walk's staged planes (the
-// walk's copies are issued and waited for here, one plane per output plane).
-// Returns false when a staged wait gave up (tmo set); every thread returns
-// the same.
-template <typename T, int G, int INTERP, bool STAGED>
-__device__ bool tps_layer(const RJob &J, int64_t Ox, int64_t Oy, int64_t zf, int zn, const TSmem<T, G> &S, Stage &st,
-                          uint32_t &parity, int &tmo, float *red, unsigned char *segf)
+// The row warps: every walk of the CTA, one output row per warp.  Returns
+// false if a wait gave up.
+template <typename T, int G, int INTERP>
+__device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
 {
     using Gm = TGeom<T, G>;
-    float4 *Nd = S.Nd;  // [4][NY][NX]   (aliases Qb)
-    float4 *Qb = S.Qb;  // [2][kTBY][NX]
-    float4 *R = S.R;    // [kTBY][4][NX]
-    const float4 *W = S.W;
-    const int tid = threadIdx.x;
-    const int tx = tid & 31, ty = tid >> 5;
-
-    // frame: the column's corner on the layer's first plane
-    const int64_t Oz = (zf / G) * G;
-    const int64_t O[3] = {Ox, Oy, Oz};
-    const int64_t c0[3] = {Ox / G, Oy / G, Oz / G};  // first node index per axis
-    const int yoff = (int)(Oy - c0[1] * G);           // rows of the first cell above the unit (G > 16)
-    const int zoff = (int)(zf - Oz);                  // first plane within the cell layer
-
-    // 1. stage node' = DF + node position - O, and the range of DF (a
-    // non-finite node forces the checked path)
-    float dmn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, dmx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
-    for (int i = tid; i < Gm::ND; i += kThreads) {
-        const int nx = i % Gm::NX, t = i / Gm::NX;
-        const int ny = t % Gm::NY, nz = t / Gm::NY;
-        int64_t gx = c0[0] + nx, gy = c0[1] + ny, gz = c0[2] + nz;
-        gx = gx < J.gsz[0] ? gx : J.gsz[0] - 1;
-        gy = gy < J.gsz[1] ? gy : J.gsz[1] - 1;
-        gz = gz < J.gsz[2] ? gz : J.gsz[2] - 1;
-        const float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
-        // node gx sits at (gx-1)*G; relative to O that is (gx-1)*G - O (exact in float)
-        float4 v;
-        v.x = d.x + (float)((gx - 1) * G - O[0]);
-        v.y = d.y + (float)((gy - 1) * G - O[1]);
-        v.z = d.z + (float)((gz - 1) * G - O[2]);
-        v.w = 0.f;
-        Nd[i] = v;
-        if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) {
-            dmn[0] = fminf(dmn[0], d.x); dmn[1] = fminf(dmn[1], d.y); dmn[2] = fminf(dmn[2], d.z);
-            dmx[0] = fmaxf(dmx[0], d.x); dmx[1] = fmaxf(dmx[1], d.y); dmx[2] = fmaxf(dmx[2], d.z);
-        } else {
-            dmn[0] = dmn[1] = dmn[2] = -3.4e38f;
-            dmx[0] = dmx[1] = dmx[2] = 3.4e38f;
-        }
-    }
-    block_minmax(dmn, dmx, red);  // contains __syncthreads (Nd visible after it)
-
-    // Sample hull: a voxel at frame position p samples p + (a convex
-    // combination of DF), so per axis q lies in [p + min DF, p + max DF].
-    const float plo[3] = {0.f, 0.f, (float)zoff};
-    const float phi[3] = {(float)(kTBX - 1), (float)(kTBY - 1), (float)(zoff + zn - 1)};
-    float mn[3], mx[3];
-    for (int a = 0; a < 3; ++a) {
-        mn[a] = dmn[a] <= -3.0e38f ? -3.4e38f : plo[a] + dmn[a];
-        mx[a] = dmx[a] >= 3.0e38f ? 3.4e38f : phi[a] + dmx[a];
-    }
-    const Frame frame = make_frame(J, O);
-    const bool span_ok = offsets_fit_32(J, mn, mx);
-    const Clamp cw = make_clamp(J, frame, mn, mx);
-
-    // 2. R[y][c][nx] = sum_b wy_b(yoff + y) Nd[c][(yoff + y)/G + b][nx]
-    for (int i = tid; i < Gm::NR; i += kThreads) {
-        const int nx = i % Gm::NX, t = i / Gm::NX;
-        const int c = t & 3, y = t >> 2;
-        const int yy = yoff + y;
-        const float4 w = W[yy % G];
-        const float4 *n0 = Nd + (c * Gm::NY + yy / G) * Gm::NX + nx;
-        const float4 a = n0[0], b = n0[Gm::NX], e = n0[2 * Gm::NX], f = n0[3 * Gm::NX];
-        float4 r;
-        r.x = fmaf(w.x, a.x, fmaf(w.y, b.x, fmaf(w.z, e.x, w.w * f.x)));
-        r.y = fmaf(w.x, a.y, fmaf(w.y, b.y, fmaf(w.z, e.y, w.w * f.y)));
-        r.z = fmaf(w.x, a.z, fmaf(w.y, b.z, fmaf(w.z, e.z, w.w * f.z)));
-        r.w = 0.f;
-        R[i] = r;
-    }
-
-    // Unchecked-path bounds per axis: every tap of a sample q with
-    // lb <= q < hb lies inside the volume and the source buffer.
-    float lb[3], hb[3];
-    for (int a = 0; a < 3; ++a) {
-        lb[a] = fmaxf(frame.lo[a], (float)frame.bl[a]) + 1.0f / 64.0f;
-        hb[a] = fminf(frame.hi[a], (float)frame.bh[a]) - 1.0f / 64.0f;
-    }
-    // per row (64 voxels): may it skip the bounds checks in x and y?  (z is
-    // decided per output plane below.)
-    const int64_t xe = J.out_o[0] + J.out_n[0] - O[0];  // valid x extent in this unit
-    const int64_t ye = J.out_o[1] + J.out_n[1] - O[1];
-    if (tid < kTBY) {
-        const int y = tid;
-        const float qx0 = dmn[0], qx1 = (float)(kTBX - 1) + dmx[0];
-        const float qy0 = (float)y + dmn[1], qy1 = (float)y + dmx[1];
-        // (rows at or beyond ye are never written, so they need no test)
-        const bool ok = (y >= ye) || (span_ok && cw.span32 && (kTBX <= xe) && qx0 >= lb[0] && qx1 < hb[0] &&
-                                      qy0 >= lb[1] && qy1 < hb[1]);
-        segf[y] = ok ? 1 : 0;
-    }
-    // plane z (at frame position pz) is unchecked in z when zlo <= pz < zhi
-    const float zlo = lb[2] - dmn[2], zhi = hb[2] - dmx[2];
-
-    const T *src = static_cast<const T *>(J.src);
-    T *dst = static_cast<T *>(J.dst);
-    const int64_t sbase = (O[2] - J.src_o[2]) * J.src_pz + (O[1] - J.src_o[1]) * J.src_py + (O[0] - J.src_o[0]);
-    // output plane z of the loop below is zf + z
-    const int64_t dbase0 = (zf - J.out_o[2]) * J.dst_pz + (O[1] - J.out_o[1]) * J.dst_py + (O[0] - J.out_o[0]);
-    BrickCtx<T> B;
-    B.base = src + sbase;
-    B.py32 = (int)J.src_py;
-    B.pz32 = (int)J.src_pz;
-    B.py = J.src_py;
-    B.pz = J.src_pz;
-    B.frame = frame;
-    B.cw = cw;
-    B.rows = make_rows(B.base, B.py32, B.pz32, cw.cl, cw.span32);
-    // x weights of the lane's voxel pair (2l, 2l+1): the unit's origin is a
-    // multiple of G (G <= 64 divides 64)
-    B.wx[0] = W[(2 * tx) % G];
-    B.wx[1] = W[(2 * tx + 1) % G];
-    B.pw = make_pairw(B.wx);
-    // a voxel pair (even x) can be written as one 2-element store
-    B.pair_ok = ((((uintptr_t)(dst + dbase0)) % (2 * sizeof(T))) == 0) && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
-    B.xe = (int)min(xe, (int64_t)kTBX);
-    B.ye = (int)min(ye, (int64_t)kTBY);
-
-    // staged window in frame coordinates (checked samples clamp into it)
-    float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
-    if (STAGED) {
-        wl[0] = (float)(-st.DX);
-        wh[0] = (float)(kBoxW - 2 - st.DX);
-        wl[1] = (float)(-st.DY);
-        wh[1] = (float)(st.rows - 2 - st.DY);
-    }
+    const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int x = 2 * lane;
+    float4 *Rw = S.Rw + y * Gm::NRW;
+    const float4 wx[2] = {S.W[x % G], S.W[(x + 1) % G]};
     const unsigned char *sm = S.base;
-    // R and the row flags are visible, and Nd (which Q overwrites) is no
-    // longer read
-    __syncthreads();
-
-    for (int z = 0; z < zn; ++z) {
-        float4 *Q = Qb + (z & 1) * (kTBY * Gm::NX);
-        const float4 wz = W[zoff + z];
-        for (int i = tid; i < kTBY * Gm::NX; i += kThreads) {
-            const int nx = i % Gm::NX, y = i / Gm::NX;
-            const float4 *r = R + (y * 4) * Gm::NX + nx;
-            const float4 a = r[0], b = r[Gm::NX], e = r[2 * Gm::NX], f = r[3 * Gm::NX];
-            float4 q;
-            q.x = fmaf(wz.x, a.x, fmaf(wz.y, b.x, fmaf(wz.z, e.x, wz.w * f.x)));
-            q.y = fmaf(wz.x, a.y, fmaf(wz.y, b.y, fmaf(wz.z, e.y, wz.w * f.y)));
-            q.z = fmaf(wz.x, a.z, fmaf(wz.y, b.z, fmaf(wz.z, e.z, wz.w * f.z)));
-            q.w = q.z;  // z twice: the packed path reads (z, z) as one pair
-            Q[i] = q;
-        }
-        // every thread is done with the previous plane (its Q buffer, and for
-        // a staged walk the slot the next copy overwrites); Q is visible
-        if (__syncthreads_or(tmo)) return false;
-        const int64_t zg = zf + z;
-        uint32_t cz = 0;
-        if (STAGED) {
-            if (st.issued < st.last) {
-                if (ty == 0) stage_issue<T, G>(J, S, st, st.issued + 1, tx);
-                ++st.issued;
+    uint32_t wslot = 0, wpar = 0;  // next ring sequence to wait for: slot, phase parity
+    uint32_t rslot = 0;            // slot of the next sequence to release
+    uint32_t k = 0;
+    for (int64_t u = blockIdx.x; u < total; u += gridDim.x, ++k) {
+        const Walk w = walk_of(jobs, njobs, u);
+        const RJob &J = jobs[w.j];
+        const uint32_t q = k & 1u;
+        if (!mbar_wait(S.splan + 8u * q, (k >> 1) & 1u, S.abort)) return false;
+        const Plan P = S.plans[q];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(S.splan + 16u + 8u * q);
+        const int64_t xe64 = J.out_o[0] + J.out_n[0] - w.Ox;
+        const int xe = (int)min(xe64, (int64_t)kTBX);
+        const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;
+        const T *src = static_cast<const T *>(J.src);
+        T *dst = static_cast<T *>(J.dst);
+        // a voxel pair (even x) can be written as one 2-element store
+        const bool pair_ok =
+            (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
+        const int Wn = P.b - P.a + 1;  // planes of a staged window
+        uint32_t waited = 0;           // sequences of this walk waited for
+        for (int64_t zf = w.z0; zf < w.z1;) {
+            const int64_t ze = min(w.z1, (zf / G + 1) * G);
+            const int64_t Oz = (zf / G) * G;
+            const int zoff = (int)(zf - Oz), zn = (int)(ze - zf);
+            RowLayer L;
+            T *drow = nullptr;
+            if (rowv) {
+                row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, S.W, Rw, wx, L);
+                drow = dst + ((zf - J.out_o[2]) * J.dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
             }
-            const int64_t sz0 = J.src_o[2];
-            if (!stage_wait<T, G>(S, st, parity, zg + st.b - sz0)) {
-                tmo = 1;
-                continue;  // the next barrier ends the unit
-            }
-            // slot of a tap plane: t = (plane - window start) + slot(window start)
-            const int64_t ws = zg + st.a - sz0;
-            const int sws = pmod(ws, Gm::R);
-            cz = (uint32_t)(int32_t)(Oz - zg - st.a + sws) - (uint32_t)kMagicBits;
-            wl[2] = (float)(zg + st.a - Oz);
-            wh[2] = (float)(zg + st.b - 1 - Oz);
-        }
-        // z of this plane: q_z lies in zoff + z + [min DF_z, max DF_z]
-        const float pz = (float)(zoff + z);
-        const bool z_fast = pz >= zlo && pz < zhi;
-        T *dslice = dst + dbase0 + (int64_t)z * J.dst_pz;
-#pragma unroll 1
-        for (int r = 0; r < kTRows; ++r) {
-            const int y = ty + kTY * r;
-            if (y >= B.ye) continue;
-            const int x = 2 * tx;
-            const bool fast = z_fast && segf[y];  // uniform across the warp (one row)
-            if (!fast && x >= B.xe) continue;
-            T *drow = dslice + (int64_t)y * J.dst_py;
-            const float4 *qn = Q + y * Gm::NX + x / G;
-            const float4 n[4] = {qn[0], qn[1], qn[2], qn[3]};
-            if constexpr (STAGED && INTERP == 0) {
-                float2 p0, p1, pz2;
-                pair_positions(n, B.pw, p0, p1, pz2);
-                if (fast) {
-                    const uint32_t w = pair_staged<T, G, true, false>(sm, st, cz, p0, p1, pz2, frame, wl, wh, 2);
-                    store_packed<T>(drow + x, w, B.pair_ok, 2);
-                } else {
-                    const int nv = B.xe - x;
-                    const uint32_t w = pair_staged<T, G, true, true>(sm, st, cz, p0, p1, pz2, frame, wl, wh, nv);
-                    store_packed<T>(drow + x, w, B.pair_ok, nv);
+            if (INTERP == 0 && P.staged) {
+                // frame (0, 0) in slot 0 minus the magic-float bias of the
+                // floor bit patterns (2^32 wrap arithmetic)
+                const uint32_t kxy = (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B +
+                                     (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
+                const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
+                for (int z = 0; z < zn; ++z) {
+                    const int64_t zg = zf + z;
+                    // the window of plane zg: sequences (zg - z0) .. (zg - z0) + Wn - 1 of the walk
+                    const uint32_t need = (uint32_t)(zg - w.z0) + (uint32_t)Wn;
+                    while (waited < need) {
+                        if (!mbar_wait(S.sfull + 8u * wslot, wpar, S.abort)) return false;
+                        ++waited;
+                        if (++wslot == (uint32_t)kRing) {
+                            wslot = 0;
+                            wpar ^= 1u;
+                        }
+                    }
+                    if (rowv) {
+                        float2 p0, p1, pz2;
+                        plane_positions(L, S.W[zoff + z], p0, p1, pz2);
+                        const float pz = (float)(zoff + z);
+                        // slot of a tap plane: t = (plane - window start) + slot(window start)
+                        const uint32_t cz = rslot + (uint32_t)(int32_t)(Oz - zg - P.a) - (uint32_t)kMagicBits;
+                        if (L.row_fast && pz >= L.zlo && pz < L.zhi) {
+                            const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
+                            const uint32_t v =
+                                pair_staged<T, false>(sm, kxy, omax, cz, p0, p1, pz2, L.frame, wl, wh, 2);
+                            store_packed<T>(drow + x, v, pair_ok, 2);
+                        } else if (x < xe) {
+                            const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(zg + P.a - Oz)};
+                            const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
+                                                 (float)(zg + P.b - 1 - Oz)};
+                            const uint32_t v =
+                                pair_staged<T, true>(sm, kxy, omax, cz, p0, p1, pz2, L.frame, wl, wh, xe - x);
+                            store_packed<T>(drow + x, v, pair_ok, xe - x);
+                        }
+                        drow += J.dst_pz;
+                    }
+                    // the window start is not read by later planes
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
+                    if (++rslot == (uint32_t)kRing) rslot = 0;
                 }
-            } else {
-                tps_pair<T, G, INTERP>(n, B, x, fast, drow);
+            } else if (rowv) {
+                Gather<T> g;
+                g.base = src + ((Oz - J.src_o[2]) * J.src_pz + (w.Oy - J.src_o[1]) * J.src_py + (w.Ox - J.src_o[0]));
+                g.py32 = (int)J.src_py;
+                g.pz32 = (int)J.src_pz;
+                g.py = J.src_py;
+                g.pz = J.src_pz;
+                g.rows = make_rows(g.base, g.py32, g.pz32, L.cw.cl, L.cw.span32);
+                for (int z = 0; z < zn; ++z) {
+                    float2 p0, p1, pz2;
+                    plane_positions(L, S.W[zoff + z], p0, p1, pz2);
+                    const float pz = (float)(zoff + z);
+                    const bool fast = L.row_fast && pz >= L.zlo && pz < L.zhi;
+                    if (fast || x < xe) gathered_pair<T, INTERP>(p0, p1, pz2, L, g, fast, xe - x, pair_ok, drow + x);
+                    drow += J.dst_pz;
+                }
+            }
+            zf = ze;
+        }
+        if (INTERP == 0 && P.staged) {
+            // the rest of the last window
+            __syncwarp();
+            for (int i = 1; i < Wn; ++i) {
+                if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
+                if (++rslot == (uint32_t)kRing) rslot = 0;
             }
         }
-    }
-    // shared memory (Nd / Q) is reused by the next layer; a wait that gave up
-    // on the last plane ends the unit here
-    return !__syncthreads_or(tmo);
-}
-
-// Plans a staged walk over output planes [z0, z1) of the column at (Ox, Oy):
-// the hull of the DF over the walk's node support gives the staged box and
-// the plane window.  false when they do not fit (every thread agrees).
-template <typename T, int G>
-__device__ bool plan_walk(const RJob &J, int64_t Ox, int64_t Oy, int64_t z0, int64_t z1, float *red, Stage &st)
-{
-    using Gm = TGeom<T, G>;
-    const int64_t cx0 = Ox / G, cy0 = Oy / G, cz0 = z0 / G;
-    const int nzn = (int)((z1 - 1) / G - cz0) + 4;
-    const int tot = Gm::NX * Gm::NY * nzn;
-    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
-    for (int i = threadIdx.x; i < tot; i += kThreads) {
-        const int nx = i % Gm::NX, t = i / Gm::NX;
-        const int ny = t % Gm::NY, nz = t / Gm::NY;
-        const int64_t gx = min(cx0 + nx, J.gsz[0] - 1), gy = min(cy0 + ny, J.gsz[1] - 1);
-        const int64_t gz = min(cz0 + nz, J.gsz[2] - 1);
-        const float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
-        if (isfinite(d.x) && isfinite(d.y) && isfinite(d.z)) {
-            mn[0] = fminf(mn[0], d.x); mn[1] = fminf(mn[1], d.y); mn[2] = fminf(mn[2], d.z);
-            mx[0] = fmaxf(mx[0], d.x); mx[1] = fmaxf(mx[1], d.y); mx[2] = fmaxf(mx[2], d.z);
-        } else {
-            mn[0] = mn[1] = mn[2] = -3.4e38f;
-            mx[0] = mx[1] = mx[2] = 3.4e38f;
-        }
-    }
-    block_minmax(mn, mx, red);
-    __syncthreads();  // `red` is written again by the next reduction
-    for (int a = 0; a < 3; ++a)
-        if (!(mn[a] > -1.0e6f && mx[a] < 1.0e6f)) return false;
-    // taps of the walk, frame coordinates: x in [fx0, 63 + fx1 + 1], y in
-    // [fy0, 15 + fy1 + 1], z in [z + fz0, z + fz1 + 1] for output plane z (a
-    // margin of 1/64 covers the FP32 rounding of the spline)
-    const float e = 1.0f / 64.0f;
-    const int fx0 = (int)floorf(mn[0] - e), fx1 = (int)floorf(mx[0] + e);
-    const int fy0 = (int)floorf(mn[1] - e), fy1 = (int)floorf(mx[1] + e);
-    const int fz0 = (int)floorf(mn[2] - e), fz1 = (int)floorf(mx[2] + e);
-    // the box's first column, in source-buffer coordinates, on a 16-byte boundary
-    constexpr int A = 16 / Gm::ES;
-    const int64_t xlo = Ox - J.src_o[0] + fx0;
-    const int64_t xhi = Ox - J.src_o[0] + kTBX + fx1;
-    const int64_t rx0 = xlo >= 0 ? (xlo / A) * A : -(((-xlo) + A - 1) / A) * A;
-    if (xhi - rx0 + 1 > kBoxW) return false;
-    const int rows = kTBY + fy1 - fy0 + 1;
-    if (rows > kHMax) return false;
-    const int a = fz0, b = fz1 + 1;
-    if (b - a + 1 + kAhead > Gm::R) return false;
-    const int64_t ry0 = Oy - J.src_o[1] + fy0;
-    const int64_t p0 = z0 + a - J.src_o[2], p1 = z1 - 1 + b - J.src_o[2];
-    const int64_t lim = (int64_t)1 << 30;  // TMA coordinates are int32
-    if (rx0 < -lim || rx0 > lim || ry0 < -lim || ry0 + rows > lim || p0 < -lim || p1 > lim) return false;
-    st.a = a;
-    st.b = b;
-    st.rx0 = (int)rx0;
-    st.ry0 = (int)ry0;
-    st.rows = rows;
-    st.DX = (int)(Ox - J.src_o[0] - rx0);
-    st.DY = -fy0;
-    return true;
-}
-
-// A staged walk over output planes [z0, z1) (planned by plan_walk).
-template <typename T, int G, int INTERP>
-__device__ bool tps_walk(const RJob &J, int64_t Ox, int64_t Oy, int64_t z0, int64_t z1, const TSmem<T, G> &S,
-                         Stage &st, uint32_t &parity, int &tmo, float *red, unsigned char *segf)
-{
-    using Gm = TGeom<T, G>;
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int64_t sz0 = J.src_o[2];
-    const uint32_t ring = 0;  // slots start at S.base
-    // offset of frame (x, y) = (0, 0) in slot 0, minus the magic-float bias
-    // of the floor bit patterns (2^32 wrap arithmetic)
-    st.kxy = ring + (uint32_t)(st.DY - kMagicBits) * (uint32_t)Gm::ROW_B +
-             (uint32_t)(st.DX - kMagicBits) * (uint32_t)Gm::ES;
-    st.omax = ring + (uint32_t)(Gm::R * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
-    const int64_t first = z0 + st.a - sz0;
-    st.last = z1 - 1 + st.b - sz0;
-    st.waited = first - 1;
-    // prologue: the first plane's window and kAhead - 1 planes beyond it
-    const int64_t pro = min(st.last, z0 + st.b + kAhead - 1 - sz0);
-    for (int64_t p = first; p <= pro; ++p)
-        if ((tid >> 5) == 0) stage_issue<T, G>(J, S, st, p, lane);
-    st.issued = pro;
-    for (int64_t zf = z0; zf < z1;) {
-        const int64_t ze = min(z1, (zf / G + 1) * G);
-        if (!tps_layer<T, G, INTERP, true>(J, Ox, Oy, zf, (int)(ze - zf), S, st, parity, tmo, red, segf))
-            return false;
-        zf = ze;
-    }
-    return true;
-}
-
-// One work unit: output planes [z0, z1) of the column at (Ox, Oy).
-template <typename T, int G, int INTERP>
-__device__ bool tps_unit(const RJob &J, int64_t Ox, int64_t Oy, int64_t z0, int64_t z1, const TSmem<T, G> &S,
-                         Stage &st, uint32_t &parity, int &tmo, float *red, unsigned char *segf)
-{
-    if (INTERP == 0 && J.tma_ok) {
-        if (plan_walk<T, G>(J, Ox, Oy, z0, z1, red, st))
-            return tps_walk<T, G, INTERP>(J, Ox, Oy, z0, z1, S, st, parity, tmo, red, segf);
-        if ((z1 - 1) / G != z0 / G) {
-            // several layers: plan each on its own
-            for (int64_t zf = z0; zf < z1;) {
-                const int64_t ze = min(z1, (zf / G + 1) * G);
-                bool ok;
-                if (plan_walk<T, G>(J, Ox, Oy, zf, ze, red, st))
-                    ok = tps_walk<T, G, INTERP>(J, Ox, Oy, zf, ze, S, st, parity, tmo, red, segf);
-                else
-                    ok = tps_layer<T, G, INTERP, false>(J, Ox, Oy, zf, (int)(ze - zf), S, st, parity, tmo, red, segf);
-                if (!ok) return false;
-                zf = ze;
-            }
-            return true;
-        }
-    }
-    for (int64_t zf = z0; zf < z1;) {
-        const int64_t ze = min(z1, (zf / G + 1) * G);
-        if (!tps_layer<T, G, INTERP, false>(J, Ox, Oy, zf, (int)(ze - zf), S, st, parity, tmo, red, segf))
-            return false;
-        zf = ze;
     }
     return true;
 }
@@ -1364,66 +1350,47 @@ __device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, 
 // ---------------------------------------------------------------- kernels
 
 template <typename T, int G, int INTERP>
-__global__ void __launch_bounds__(kThreads, 2) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
-                                                               int64_t total_units, int *err)
+__global__ void __maxnreg__(120) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
+                                                                  int64_t total_units, int *err)
 {
     using Gm = TGeom<T, G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ float red[6 * (kThreads / 32)];
-    __shared__ unsigned char segf[kTBY];
+    __shared__ int abort_sh;
     // ring slots first, on a 128-byte boundary (TMA destinations), then the
-    // slots' mbarriers, then the node / R / Q / weight arrays
+    // mbarriers, the plans, the weight table and the row warps' node rows
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t pad = (128u - (raw & 127u)) & 127u;
-    TSmem<T, G> S;
+    TSmem S;
     S.base = smem_raw + pad;
     S.sring = raw + pad;
-    S.smbar = S.sring + (uint32_t)Gm::RING_B;
-    float4 *f4 = reinterpret_cast<float4 *>(S.base + Gm::RING_B + Gm::MBAR_B);
-    S.Nd = f4;
-    S.Qb = f4;
-    S.R = f4 + Gm::UNION;
-    S.W = S.R + Gm::NR;
+    S.sfull = S.sring + (uint32_t)Gm::RING_B;
+    S.splan = S.sfull + 16u * kRing;
+    unsigned char *tail = S.base + Gm::RING_B + 8 * Gm::NBAR;
+    S.plans = reinterpret_cast<Plan *>(tail);
+    S.W = reinterpret_cast<float4 *>(tail + 2 * sizeof(Plan));
+    S.Rw = S.W + G;
+    S.abort = &abort_sh;
     const int tid = threadIdx.x;
     if (tid < G) S.W[tid] = bspline_w(tid, G);
-    if (tid < Gm::R) mbar_init(S.smbar + 8u * (uint32_t)tid, 1);
-    if (tid == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    __syncthreads();
-    uint32_t parity = 0;  // bit s: parity of the next phase of slot s's mbarrier
-    int tmo = 0;
-    Stage st;
-    st.a = st.b = st.rx0 = st.ry0 = st.rows = st.DX = st.DY = 0;
-    st.issued = st.waited = st.last = 0;
-    st.kxy = st.omax = 0;
-    int last_job = -1;
-    bool aborted = false;
-    for (int64_t u = blockIdx.x; u < total_units; u += gridDim.x) {
-        const int j = find_job(jobs, njobs, u);
-        const RJob &J = jobs[j];
-        if (INTERP == 0 && j != last_job && J.tma_ok && tid < 32)  // the descriptor was written by a copy
-            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
-        last_job = j;
-        const int64_t lu = u - J.brick_begin;
-        const int64_t bx = lu % J.bricks[0], t = lu / J.bricks[0];
-        const int64_t by = t % J.bricks[1], bz = t / J.bricks[1];
-        const int64_t Ox = J.out_o[0] + bx * kTBX, Oy = J.out_o[1] + by * kTBY;
-        const int64_t z0 = J.out_o[2] + bz * J.zs;
-        const int64_t z1 = min(z0 + (int64_t)J.zs, J.out_o[2] + J.out_n[2]);
-        if (!tps_unit<T, G, INTERP>(J, Ox, Oy, z0, z1, S, st, parity, tmo, red, segf)) {
-            aborted = true;
-            break;
-        }
+    if (tid < kRing) {
+        mbar_init(S.sfull + 8u * tid, 1);
+        mbar_init(S.sfull + 8u * (kRing + tid), kRowWarps);
     }
-    if (aborted && tid == 0) {
-        if (err) atomicOr(err, kKernErrTimeout);
-        // let the copies still in flight land (each wait bounded) before the CTA exits
-        while (st.waited < st.issued) {
-            const int64_t p = st.waited + 1;
-            const int s = pmod(p, Gm::R);
-            if (!mbar_wait(S.smbar + 8u * (uint32_t)s, (parity >> s) & 1u)) break;
-            parity ^= 1u << s;
-            st.waited = p;
-        }
+    if (tid < 2) {
+        mbar_init(S.splan + 8u * tid, 1);
+        mbar_init(S.splan + 16u + 8u * tid, kRowWarps);
+    }
+    if (tid == 0) {
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = (tid >> 5) == kRowWarps ? tps_copier<T, G, INTERP>(jobs, njobs, total_units, S)
+                                            : tps_rows<T, G, INTERP>(jobs, njobs, total_units, S);
+    if (!ok) {
+        // the other warps see the flag in their waits and return
+        *reinterpret_cast<volatile int *>(&abort_sh) = 1;
+        if ((tid & 31) == 0 && err) atomicOr(err, kKernErrTimeout);
     }
 }
 
@@ -1451,17 +1418,14 @@ cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_
     auto k = k_resample_tps<T, G, INTERP>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
     if (e != cudaSuccess) return e;
-    // two CTAs per SM need the largest shared-memory carveout
-    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, Gm::smem_bytes);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTpsThreads, Gm::smem_bytes);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int64_t grid = (int64_t)sms * per_sm;
     if (grid > total) grid = total;
     if (grid < 1) grid = 1;
-    k<<<(unsigned)grid, kThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, err);
+    k<<<(unsigned)grid, kTpsThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, err);
     return cudaGetLastError();
 }
 

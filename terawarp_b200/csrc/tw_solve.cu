@@ -302,13 +302,9 @@ __device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status, unsigned l
     return ok_sh != 0;
 }
 
-// potrf of diagonal block kb in shared memory, by one warp: lane l owns rows
-// l and l + 32.  In step j the owners of rows below j scale their element of
-// column j by rsqrt(pivot) and keep it in a register, then update their rows'
-// elements of the trailing lower triangle, column by column, from that
-// register and the (broadcast) scaled element of the column's own row.  The
-// warp synchronises with __syncwarp only, so a block costs no CTA barriers
-// beyond the two around it (the other warps wait there).
+// potrf of diagonal block kb in shared memory: in step j threads j..63 take
+// the pivot (x rsqrt(d)) and scale column j, then each thread updates its 4 x 4
+// patch of the trailing lower triangle from register copies of the column.
 __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, double *sm)
 {
     double(*a)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
@@ -322,30 +318,40 @@ __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, d
         a[r][c] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
     }
     __syncthreads();
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        const int i0 = lane, i1 = lane + 32;
-        for (int j = 0; j < kNB; ++j) {
+    const int t = threadIdx.x;
+    // thread t updates rows tr + 16u and columns tc + 16v of the block: the
+    // 16 threads of a half-warp then read 16 consecutive rows of a column
+    // (distinct banks with the 65-double row pitch)
+    const int tr = t >> 4, tc = t & 15;
+    for (int j = 0; j < kNB; ++j) {
+        if (t >= j && t < kNB) {
             double d = a[j][j];
             if (!(d > 0.0)) {
-                if (lane == 0) atomicOr(status, kStNotSPD);
+                if (t == j) atomicOr(status, kStNotSPD);
                 d = 1.0;
             }
             const double inv = rsqrt(d);
-            double c0 = 0.0, c1 = 0.0;
-            if (i0 > j) { c0 = a[i0][j] * inv; a[i0][j] = c0; }
-            if (i1 > j) { c1 = a[i1][j] * inv; a[i1][j] = c1; }
-            if (lane == 0) sd[j] = d * inv;
-            __syncwarp();
-            for (int l = j + 1; l < kNB; ++l) {
-                const double cl = a[l][j];
-                if (i0 >= l) a[i0][l] -= c0 * cl;
-                if (i1 >= l) a[i1][l] -= c1 * cl;
-            }
-            __syncwarp();
+            if (t == j) sd[j] = d * inv;
+            else a[t][j] *= inv;
         }
+        __syncthreads();
+        if (tr + 48 > j) {
+            double ci[4], cl[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                ci[u] = a[tr + 16 * u][j];
+                cl[u] = a[tc + 16 * u][j];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int i = tr + 16 * u, l = tc + 16 * v;
+                    if (l > j && i >= l) a[i][l] -= ci[u] * cl[v];
+                }
+        }
+        __syncthreads();
     }
-    __syncthreads();
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
         int r = e / kNB, c = e % kNB;
         if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c < r ? a[r][c] : (c == r ? sd[r] : 0.0);
