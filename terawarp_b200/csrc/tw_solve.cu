@@ -232,29 +232,42 @@ __global__ void k_fill_a(const double *__restrict__ ctr, int n, const double *__
 
 // ---- 3b-4b: one cooperative kernel, one CTA of 256 threads per SM.
 //
-// The blocked right-looking Cholesky runs as phases separated by grid-wide
-// barriers: for each column block kb, CTA 0 factors the diagonal block
-// (potrf), every CTA takes row blocks of the panel (trsm), every CTA takes
-// 64 x 64 tiles of the trailing update (syrk).  The back substitution then
-// alternates CTA 0 solving a diagonal block with every CTA updating the rows
-// above it.  A phase is short (tens of microseconds), so a barrier instead
-// of a kernel launch per phase removes ~200 launches per solve.  L1 is not
-// coherent across SMs within a kernel, so every load of data another CTA may
-// have written in an earlier phase (A, z) bypasses L1 (__ldcg).
+// The tiled right-looking Cholesky and both substitutions run as tasks on
+// 64 x 64 tiles, ordered by dependency counters in global memory instead of
+// grid-wide barriers: POTRF(k) factors diagonal tile k once every update of
+// it has landed; TRSM(i, k) solves row block i of panel k (the right-hand-side
+// block included) once POTRF(k) and the updates of tile (i, k) are done;
+// UPDATE(i, j, k) subtracts L(i,k) L(j,k)' from tile (i, j) once both panel
+// tiles exist and the tile's previous update is in.  The back substitution
+// is DIAG(kb) (the diagonal block's triangular solve) and BACK(ib, kb) (the
+// rows of block ib) in the same way.  Tasks are numbered in one order that
+// respects every dependency (step by step; within a step POTRF, the panel,
+// then the updates column by column, so the next panel's tiles come first),
+// and CTA c takes tasks c, c + G, c + 2G, ... in that order; as all CTAs are
+// resident (cooperative launch), the lowest unfinished task can always run,
+// so the schedule cannot deadlock.  A step's critical path is then one
+// POTRF, one TRSM and one UPDATE instead of two grid-wide barriers, and
+// later steps start while earlier ones finish.  L1 is not coherent across
+// SMs within a kernel, so every load of data another CTA wrote (A, z)
+// bypasses L1 (__ldcg).
 
 constexpr int kSolveThreads = 256;
 constexpr int kStTimeout = 4;
-// A CTA gives up on a barrier after limit_ns (the context's
+// A CTA gives up on a dependency after limit_ns (the context's
 // solve_barrier_ns, 30 s unless a test shortened it).  The launch is
 // cooperative, so every CTA can be resident at once; while other work (the
 // previous job's resample, a caller's kernel on another stream) still holds
 // SMs, some CTAs start later than others and the early ones wait, so the
 // bound is generous, but it is a bound.
 
-struct GridBar {
-    unsigned int count;   // CTAs arrived at the current barrier
-    unsigned int gen;     // barriers completed
-    int err;              // set by a CTA that gave up waiting
+// Dependency counters (zeroed before the launch); tdone[nblk + 1] (panel
+// tiles solved per row block), cnt[(nblk + 1) nblk] (updates applied per
+// tile) and bcnt[nblk] (back-substitution updates applied per row block)
+// follow in the same allocation.
+struct SolveFlags {
+    int err;    // set by a CTA that gave up waiting
+    int pdone;  // diagonal tiles factored
+    int ddone;  // back-substitution diagonal blocks solved, from the last block down
     int pad;
 };
 
@@ -265,41 +278,52 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     return t;
 }
 
-// Grid-wide barrier with a bounded wait.  `gen` is the caller's count of
-// barriers passed (kept by thread 0).  Returns false, on every thread of the
-// CTA, if this or another CTA gave up; the caller then returns.
-__device__ bool grid_sync(GridBar *b, unsigned int &gen, int *status, unsigned long long limit_ns)
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Thread 0 waits until *flag >= want; every thread returns true, or false
+// (on every thread) when this or another CTA gave up.
+__device__ bool wait_ge(const int *flag, int want, SolveFlags *F, int *status, unsigned long long limit_ns)
 {
     __shared__ int ok_sh;
-    __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned int g = gen;
-        __threadfence();
-        if (atomicAdd(&b->count, 1u) + 1u == gridDim.x) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicExch(&b->gen, g + 1u);
-        } else {
+        if (ld_acquire(flag) < want) {
             const unsigned long long t0 = globaltimer_ns();
-            while (*reinterpret_cast<volatile unsigned int *>(&b->gen) == g) {
-                if (*reinterpret_cast<volatile int *>(&b->err) ||
-                    globaltimer_ns() - t0 > limit_ns) {
-                    atomicOr(&b->err, 1);
+            while (ld_acquire(flag) < want) {
+                if (*reinterpret_cast<volatile int *>(&F->err) || globaltimer_ns() - t0 > limit_ns) {
+                    atomicOr(&F->err, 1);
                     atomicOr(status, kStTimeout);
                     ok = 0;
                     break;
                 }
-                __nanosleep(100);
+                __nanosleep(32);
             }
         }
         __threadfence();
-        gen = g + 1u;
-        if (*reinterpret_cast<volatile int *>(&b->err)) ok = 0;
         ok_sh = ok;
     }
     __syncthreads();
     return ok_sh != 0;
+}
+
+// Publishes a finished task: every thread's writes, then *flag = value.
+__device__ __forceinline__ void signal_done(int *flag, int value)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        st_release(flag, value);
+    }
 }
 
 // potrf of diagonal block kb in shared memory: in step j threads j..63 take
@@ -412,21 +436,14 @@ __device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double 
     }
 }
 
-// syrk tile number t of step kb: A(ib,jb) -= L(ib,kb) L(jb,kb)' for
+// Trailing update of tile (ib, jb) at step kb: A(ib,jb) -= L(ib,kb) L(jb,kb)' for
 // kb < jb <= ib, jb a column block and ib a row block (the right-hand-side
-// block included), t enumerating the pairs; each thread owns a 4 x 4 patch.
-__device__ void syrk_tile(double *__restrict__ A, int m, int kb, long long t, double *sm)
+// block included); each thread owns a 4 x 4 patch.
+__device__ void syrk_tile(double *__restrict__ A, int m, int kb, int ib, int jb, double *sm)
 {
     double(*Li)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
     double(*Lj)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
     const int nblk = (m + kNB - 1) / kNB;
-    // invert t = ib'(ib'+1)/2 + jb' (0 <= jb' <= ib')
-    int ibp = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((long long)(ibp + 1) * (ibp + 2) / 2 <= t) ++ibp;
-    while ((long long)ibp * (ibp + 1) / 2 > t) --ibp;
-    const int jbp = (int)(t - (long long)ibp * (ibp + 1) / 2);
-    const int ib = kb + 1 + ibp, jb = kb + 1 + jbp;
-    if (jb >= nblk) return;  // the right-hand-side block has no diagonal tile
     const int r0 = kb * kNB, i0 = row_block_start(ib, nblk, m), j0 = jb * kNB;
     const int nbk = min(kNB, m - r0), nbi = row_block_rows(ib, nblk, m), nbj = min(kNB, m - j0);
     __syncthreads();
@@ -499,51 +516,103 @@ __device__ void bwd_diag(const double *__restrict__ A, int m, int kb, double *__
     }
 }
 
+// Back substitution, rows of block ib: z(ib) -= L(kb, ib)' x(kb), x(kb)
+// already in z(kb); thread (row, rhs) accumulates over the 64 rows of L(kb, .)
+// in order.
+__device__ void bwd_update(const double *__restrict__ A, int m, int kb, int ib, double *__restrict__ z, double *sm)
+{
+    const int r0 = kb * kNB, nb = min(kNB, m - r0);
+    const int i0 = ib * kNB, nbi = min(kNB, m - i0);
+    double *x = sm;  // x(kb), 64 x 4
+    __syncthreads();
+    for (int e = threadIdx.x; e < 4 * nb; e += blockDim.x) x[e] = __ldcg(&z[r0 * 4 + e]);
+    __syncthreads();
+    const int il = threadIdx.x >> 2, r = threadIdx.x & 3;
+    if (il < nbi) {
+        double s = 0.0;
+#pragma unroll 16
+        for (int p = 0; p < nb; ++p) s += __ldcg(&A[(size_t)(r0 + p) * m + i0 + il]) * x[p * 4 + r];
+        double *zi = &z[(i0 + il) * 4 + r];
+        *zi = __ldcg(zi) - s;
+    }
+}
+
 __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict__ A, int m, double *__restrict__ Z,
-                                                              int *status, GridBar *bar, unsigned long long limit_ns)
+                                                              int *status, int *flags, unsigned long long limit_ns)
 {
     extern __shared__ double sm[];
-    unsigned int gen = 0;
     const int nblk = (m + kNB - 1) / kNB;
-    if (blockIdx.x == 0) potrf_tile(A, m, 0, status, sm);
-    if (!grid_sync(bar, gen, status, limit_ns)) return;
-    for (int kb = 0; kb < nblk; ++kb) {
-        const int rest = nblk - kb - 1;
-        // row blocks below the diagonal: the rest of A plus the right-hand-side block
-        for (int b = blockIdx.x; b < rest + 1; b += gridDim.x) trsm_tile(A, m, kb, kb + 1 + b, sm);
-        if (!grid_sync(bar, gen, status, limit_ns)) return;
-        // Lookahead: tile 0 of the trailing update is the next diagonal block
-        // (kb+1, kb+1), which no other tile of this step touches; CTA 0 updates
-        // it first and factors it at once, while the other CTAs are still on
-        // their tiles, so the next step needs no potrf phase of its own.
-        const long long pairs = (long long)(rest + 1) * (rest + 2) / 2;
-        for (long long t = blockIdx.x; t < pairs; t += gridDim.x) {
-            syrk_tile(A, m, kb, t, sm);
-            if (t == 0 && rest > 0) potrf_tile(A, m, kb + 1, status, sm);
-        }
-        if (!grid_sync(bar, gen, status, limit_ns)) return;
-    }
-    // y' sits in rows m..m+3; back substitution L' x = y into Z rows 4..n-1
-    double *z = Z + 16;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
-    for (int e = gt; e < 4 * m; e += gstride) z[e] = __ldcg(&A[(size_t)(m + (e & 3)) * m + (e >> 2)]);
-    if (!grid_sync(bar, gen, status, limit_ns)) return;
-    for (int kb = nblk - 1; kb >= 0; --kb) {
-        if (blockIdx.x == 0) bwd_diag(A, m, kb, z, sm);
-        if (!grid_sync(bar, gen, status, limit_ns)) return;
-        const int r0 = kb * kNB, nb = min(kNB, m - r0);
-        for (int i = gt; i < r0; i += gstride) {
-            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-#pragma unroll 8
-            for (int p = 0; p < nb; ++p) {
-                const double l = __ldcg(&A[(size_t)(r0 + p) * m + i]);
-                const double *xp = z + (r0 + p) * 4;
-                s0 += l * __ldcg(xp); s1 += l * __ldcg(xp + 1); s2 += l * __ldcg(xp + 2); s3 += l * __ldcg(xp + 3);
+    SolveFlags *F = reinterpret_cast<SolveFlags *>(flags);
+    int *tdone = flags + 4;
+    int *cnt = tdone + nblk + 1;
+    int *bcnt = cnt + (nblk + 1) * nblk;
+    double *z = Z + 16;  // z(4:), 4 per row; y' then x' overwrite it
+    const long long G = gridDim.x, bid = blockIdx.x;
+    long long base = 0;  // number of the step's first task
+    for (int k = 0; k < nblk; ++k) {
+        const int nt = nblk - k;  // panel tiles: row blocks k+1 .. nblk
+        long long nu = 0;         // updates: column blocks j = k+1 .. nblk-1, row blocks j .. nblk
+        for (int j = k + 1; j < nblk; ++j) nu += nblk + 1 - j;
+        const long long count = 1 + nt + nu;
+        for (long long e = ((bid - base) % G + G) % G; e < count; e += G) {
+            if (e == 0) {
+                if (!wait_ge(&cnt[k * nblk + k], k, F, status, limit_ns)) return;
+                potrf_tile(A, m, k, status, sm);
+                signal_done(&F->pdone, k + 1);
+            } else if (e <= nt) {
+                const int i = k + (int)e;
+                if (!wait_ge(&F->pdone, k + 1, F, status, limit_ns) ||
+                    !wait_ge(&cnt[i * nblk + k], k, F, status, limit_ns))
+                    return;
+                trsm_tile(A, m, k, i, sm);
+                if (i == nblk) {
+                    // y' of block k is final: seed z(k) for the back substitution
+                    __syncthreads();
+                    const int r0 = k * kNB, nb = min(kNB, m - r0);
+                    for (int q = threadIdx.x; q < 4 * nb; q += blockDim.x)
+                        z[(r0 + (q >> 2)) * 4 + (q & 3)] = __ldcg(&A[(size_t)(m + (q & 3)) * m + r0 + (q >> 2)]);
+                }
+                signal_done(&tdone[i], k + 1);
+            } else {
+                long long f = e - 1 - nt;
+                int j = k + 1;
+                while (f >= nblk + 1 - j) {
+                    f -= nblk + 1 - j;
+                    ++j;
+                }
+                const int i = j + (int)f;
+                if (!wait_ge(&tdone[i], k + 1, F, status, limit_ns) ||
+                    !wait_ge(&tdone[j], k + 1, F, status, limit_ns) ||
+                    !wait_ge(&cnt[i * nblk + j], k, F, status, limit_ns))
+                    return;
+                syrk_tile(A, m, k, i, j, sm);
+                signal_done(&cnt[i * nblk + j], k + 1);
             }
-            double *zi = z + i * 4;
-            zi[0] = __ldcg(zi) - s0; zi[1] = __ldcg(zi + 1) - s1; zi[2] = __ldcg(zi + 2) - s2; zi[3] = __ldcg(zi + 3) - s3;
         }
-        if (!grid_sync(bar, gen, status, limit_ns)) return;
+        base += count;
+    }
+    // back substitution L' x = y, block by block from the last: DIAG(kb)
+    // needs y'(kb) (TRSM(nblk, kb)) and every BACK(kb, kb') for kb' > kb;
+    // BACK(ib, kb) needs DIAG(kb) and the block's previous BACK
+    for (int kb = nblk - 1; kb >= 0; --kb) {
+        const long long count = 1 + kb;  // DIAG(kb), then BACK(ib, kb) for ib = kb-1 .. 0
+        for (long long e = ((bid - base) % G + G) % G; e < count; e += G) {
+            if (e == 0) {
+                if (!wait_ge(&tdone[nblk], kb + 1, F, status, limit_ns) ||
+                    !wait_ge(&bcnt[kb], nblk - 1 - kb, F, status, limit_ns))
+                    return;
+                bwd_diag(A, m, kb, z, sm);
+                signal_done(&F->ddone, nblk - kb);
+            } else {
+                const int ib = kb - (int)e;
+                if (!wait_ge(&F->ddone, nblk - kb, F, status, limit_ns) ||
+                    !wait_ge(&bcnt[ib], nblk - 1 - kb, F, status, limit_ns))
+                    return;
+                bwd_update(A, m, kb, ib, z, sm);
+                signal_done(&bcnt[ib], nblk - kb);
+            }
+        }
+        base += count;
     }
 }
 
@@ -738,8 +807,11 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
 {
     const int m = n - 4;
     // workspace: ctr 3n, Y 4n, Xw 4n, V 4n, P 4n, W 4n, Z 4n, KC 4n, tau 4, R 16, d 16, status
-    // ctr 3n, Y/Xw/V/P/W/Z/KC 4n each, tau 4, R 16, grid barrier 2
-    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + 2;
+    // ctr 3n, Y/Xw/V/P/W/Z/KC 4n each, tau 4, R 16, then the solve kernel's
+    // dependency counters (ints)
+    const int nblk = m > 0 ? (m + kNB - 1) / kNB : 0;
+    const size_t nflags = 4 + (size_t)(nblk + 1) + (size_t)(nblk + 1) * nblk + (size_t)nblk;
+    const size_t small = 3 * (size_t)n + 7 * 4 * (size_t)n + 4 + 16 + (nflags + 1) / 2;
     // stream-ordered workspace on `st`, returned to the pool on `st` when this
     // function exits (after the final wait, or with the error)
     StreamBuf ws{ctx, st}, abuf{ctx, st};
@@ -758,7 +830,7 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
     double *d_R = d_tau + 4;
     double *d_d = d_d_out;
     int *d_status = d_status_out;
-    GridBar *d_bar = reinterpret_cast<GridBar *>(d_R + 16);  // 16 bytes, 8-byte aligned
+    int *d_flags = reinterpret_cast<int *>(d_R + 16);
     if (m > 0) {
         abuf.bytes = (size_t)(m + 4) * m * sizeof(double);
         TW_TRY(dmalloc_on(ctx, &abuf.p, abuf.bytes, st));
@@ -801,9 +873,9 @@ tw_status solve_tps_device(tw_ctx *ctx, const double *h_ctr, const double *h_val
         TW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_solve, kSolveThreads, kSolveSmem));
         if (per_sm < 1) return fail(ctx, TW_ERR_CUDA, "solve kernel does not fit on an SM");
         int grid = ctx->sm_count;
-        TW_CUDA_TRY(cudaMemsetAsync(d_bar, 0, sizeof(GridBar), st));
+        TW_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * nflags, st));
         unsigned long long limit_ns = ctx->solve_barrier_ns.load();
-        void *args[] = {(void *)&d_A, (void *)&m, (void *)&d_Z, (void *)&d_status, (void *)&d_bar, (void *)&limit_ns};
+        void *args[] = {(void *)&d_A, (void *)&m, (void *)&d_Z, (void *)&d_status, (void *)&d_flags, (void *)&limit_ns};
         TW_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_chol_solve, dim3(grid), dim3(kSolveThreads), args,
                                                 kSolveSmem, st));
         ++nl;
@@ -831,7 +903,7 @@ tw_status solve_status(tw_ctx *ctx, const int *d_status, cudaStream_t st)
     if (status & kStSingularX)
         return fail(ctx, TW_ERR_SINGULAR, "TPS centres are degenerate: [1 s] is rank deficient (coplanar or < 4 distinct points)");
     if (status & kStTimeout)
-        return fail(ctx, TW_ERR_TIMEOUT, "TPS solve: a grid barrier timed out");
+        return fail(ctx, TW_ERR_TIMEOUT, "TPS solve: a wait on another block of the solve timed out");
     if (status & kStNotSPD)
         return fail(ctx, TW_ERR_SINGULAR, "projected TPS system is not positive definite");
     return TW_OK;
