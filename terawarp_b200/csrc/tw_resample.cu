@@ -552,28 +552,29 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // position and value do not depend on how the volume is cut into units or
 // how units are batched.
 //
-// A CTA is 16 row warps and one copy warp.  Row warp w owns output row w of
-// the unit; lane l owns the voxel pair (2l, 2l+1), so a warp covers one whole
-// 64-voxel row.  Per cell layer a row warp contracts the 4 x 4 x (64/G + 3)
-// nodes of its row along y (into warp-private shared memory), then every
-// lane contracts them along x for its voxel pair: four (one per node layer
-// along z) position pairs P_c kept in registers.  Per output plane the
-// positions are sum_c wz_c P_c (12 FFMA2 per pair); no node data is touched
-// and no barrier is taken.
+// A CTA is 16 warps, one per output row of the unit; lane l owns the voxel
+// pair (2l, 2l+1), so a warp covers one whole 64-voxel row.  Per cell layer a
+// warp contracts the 4 x 4 x (64/G + 3) nodes of its row along y (into
+// warp-private shared memory), then every lane contracts them along x for
+// its voxel pair: four (one per node layer along z) position pairs P_c kept
+// in registers.  Per output plane the positions are sum_c wz_c P_c (12 FFMA2
+// per pair); no node data is touched and no barrier is taken.
 //
 // Staged walks.  The column's source footprint over a walk -- the convex
 // hull of its nodes' displacements (B-spline weights are >= 0 and sum to 1)
 // plus the +1 tap -- is a box of at most kBoxW x kHMax elements per source
 // plane and a window of W planes that slides down one plane per output
-// plane.  The copy warp plans each walk, publishes the plan, and copies the
+// plane.  Warp 0 also plans each walk, publishes the plan, and copies the
 // box's rows of every source plane the walk reads, in order, into a ring of
 // kRing plane slots by TMA (cp.async.bulk.tensor, one row per copy, from this
 // GPU's own memory; no multicast).  Each slot has a "full" mbarrier
 // (transaction count of the copies) and an "empty" mbarrier (one arrival per
-// row warp once no later plane of that warp reads the slot): the copy warp
-// refills a slot as soon as every row warp has released it, so copies run
-// up to kRing - W planes ahead of the slowest row warp and row warps never
-// wait for one another.  Slot 0 is copied a second time past the last slot,
+// warp once no later plane of that warp reads the slot).  Warp 0 never blocks
+// on its copier role: between its own planes, and while it waits, it issues
+// every copy whose slot has been released by all warps (and plans walks as
+// the copies reach them), so copies run up to kRing - W planes ahead of the
+// slowest warp and no warp waits for another except through the data.
+// Slot 0 is copied a second time past the last slot,
 // so the z+1 tap of any plane is at a fixed offset.  The slots' row pitch is
 // 128 elements: a row or plane step moves an address by a multiple of 32
 // banks, so a warp's loads hit distinct banks whichever rows and planes its
@@ -583,9 +584,10 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // (trilerp2).
 
 constexpr int kTBX = 64;                     // unit width (x): 32 lanes x 2 voxels
-constexpr int kTBY = 16;                     // unit height (y): one row warp per row
+constexpr int kTBY = 16;                     // unit height (y): one warp per row
 constexpr int kRowWarps = kTBY;
-constexpr int kTpsThreads = 32 * (kRowWarps + 1);  // + the copy warp
+constexpr int kTpsThreads = 32 * kRowWarps;
+constexpr int kPlans = 4;                    // plan slots: walks planned ahead of the slowest warp
 constexpr int kBoxW = kStageBoxW;            // TMA box: source elements per row copy
 constexpr int kRowP = 128;                   // shared-memory row pitch (elements)
 constexpr int kHMax = 28;                    // staged rows per plane
@@ -595,7 +597,7 @@ constexpr int kMinAhead = 2;                 // slots a walk's window leaves for
 // an error (the kernel reports kKernErrTimeout and returns)
 constexpr unsigned long long kStageWaitNs = 2000000000ull;
 
-// A walk's staging plan, written by the copy warp, read by the row warps.
+// A walk's staging plan, written by warp 0, read by every warp.
 struct alignas(16) Plan {
     int staged;    // 1: the walk's source footprint is staged
     int a, b;      // output plane z reads source planes [z + a, z + b]
@@ -606,6 +608,21 @@ struct alignas(16) Plan {
     int pad[3];
 };
 
+// Warp 0's copier state: the walk it is planning or copying (the copy
+// frontier) and the ring position of the next copy.
+struct alignas(16) CopyState {
+    int64_t u;        // flattened unit index of the frontier walk (>= total: done)
+    int64_t pfirst;   // buffer z of the frontier walk's first staged plane
+    uint32_t k;       // walk number of the frontier walk (its plan slot is k % kPlans)
+    int planned;      // the frontier walk's plan is published
+    int i;            // next plane of the frontier walk to copy
+    int j;            // job of the frontier walk
+    int last_job;     // job whose tensor map was last acquired
+    uint32_t seq;     // planes copied so far
+    uint32_t slot;    // seq % kRing
+    int pad;
+};
+
 template <typename T, int G>
 struct TGeom {
     static constexpr int NX = kTBX / G + 3;       // node columns of a unit (G <= 64)
@@ -614,10 +631,11 @@ struct TGeom {
     static constexpr int ROW_B = kRowP * ES;
     static constexpr int PLANE_B = kHMax * ROW_B;
     static constexpr int RING_B = (kRing + 1) * PLANE_B;
-    static constexpr int NBAR = 2 * kRing + 4;    // full[kRing], empty[kRing], plan full[2], plan empty[2]
-    static constexpr size_t smem_bytes =
-        128 + (size_t)RING_B + 8 * NBAR + 2 * sizeof(Plan) + sizeof(float4) * (size_t)(G + kRowWarps * NRW);
-    static_assert((8 * NBAR) % 16 == 0, "the weight table is float4-aligned");
+    static constexpr int NBAR = 2 * kRing + 2 * kPlans;  // full[kRing], empty[kRing], plan full / empty[kPlans]
+    static constexpr size_t smem_bytes = 128 + (size_t)RING_B + 8 * NBAR + kPlans * sizeof(Plan) + sizeof(CopyState) +
+                                         sizeof(float4) * (size_t)(G + kRowWarps * NRW);
+    static_assert((8 * NBAR) % 16 == 0 && sizeof(Plan) % 16 == 0 && sizeof(CopyState) % 16 == 0,
+                  "the weight table is float4-aligned");
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
@@ -689,8 +707,9 @@ struct TSmem {
     unsigned char *base;  // 128-byte aligned start of the ring
     uint32_t sring;       // shared-window address of slot 0
     uint32_t sfull;       // shared-window address of full[0] (8 bytes each); empty[s] = full[s] + 8 kRing
-    uint32_t splan;       // plan full[0..1], then plan empty[0..1]
-    Plan *plans;          // two plan slots
+    uint32_t splan;       // plan full[0 .. kPlans-1], then plan empty[0 .. kPlans-1]
+    Plan *plans;          // kPlans plan slots
+    CopyState *cs;        // warp 0's copier state
     float4 *W;            // B-spline weights at t = i / G
     float4 *Rw;           // per row warp: y-contracted nodes of its row
     int *abort;           // set by a warp that gave up waiting
@@ -793,91 +812,106 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     return P;
 }
 
-// The copy warp: plans every walk of the CTA, publishes each plan, and
-// copies each staged walk's source planes into the ring, in order.  Returns
-// false if a wait gave up.
+// Warp 0's copier role, never blocking: plans and publishes walks and
+// issues plane copies, in ring order, for as long as plan slots and ring
+// slots are free (released by every warp).  Called by warp 0 between its
+// planes and while it waits.
 template <typename T, int G, int INTERP>
-__device__ bool tps_copier(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
+__device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
 {
     using Gm = TGeom<T, G>;
     const int lane = threadIdx.x & 31;
-    uint32_t seq = 0;  // source planes copied so far (ring sequence number)
-    uint32_t slot = 0;
-    int last_job = -1;
-    int64_t u = blockIdx.x;
-    if (u >= total) return true;
-    Walk w = walk_of(jobs, njobs, u);
-    auto plan_of = [&](const Walk &wk) -> Plan {
-        const RJob &J = jobs[wk.j];
-        if (INTERP != 0 || !J.tma_ok) return Plan{};
-        if (wk.j != last_job)  // the descriptor was written by a copy
-            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
-        last_job = wk.j;
-        return plan_walk<T, G>(J, wk);
-    };
-    Plan nxt = plan_of(w);
-    bool ok = true;
-    for (uint32_t k = 0;; ++k) {
-        const Plan P = nxt;
-        const RJob &J = jobs[w.j];
-        // publish the plan (its slot is free once every row warp has read
-        // the plan two walks back)
-        const uint32_t q = k & 1u;
-        if (k >= 2 && !mbar_wait(S.splan + 16u + 8u * q, ((k >> 1) - 1u) & 1u, S.abort)) { ok = false; break; }
-        if (lane == 0) S.plans[q] = P;
-        __syncwarp();
-        if (lane == 0) mbar_arrive(S.splan + 8u * q);
-        const int64_t un = u + gridDim.x;
-        const bool more = un < total;
-        Walk wn = w;
-        if (more) wn = walk_of(jobs, njobs, un);
-        bool planned = !more;
-        // copy the walk's planes; the next walk is planned once this walk's
-        // first window is on its way
-        const int64_t pfirst = w.z0 + P.a - J.src_o[2];
-        const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)P.rows;
-        for (int i = 0; i < P.nplanes; ++i) {
-            if (!planned && i == P.b - P.a + 1) {
-                nxt = plan_of(wn);
-                planned = true;
+    CopyState &C = *S.cs;
+    // bounded work per call: a ring's worth of copies and a few walks
+    for (int step = 0; step < kRing + 2 * kPlans; ++step) {
+        __syncwarp();  // lane 0's last update of C is visible
+        const int64_t u = C.u;
+        if (u >= total) return;
+        const uint32_t k = C.k, q = k % kPlans;
+        if (!C.planned) {
+            // the plan slot is free once every warp has read the plan kPlans walks back
+            if (k >= (uint32_t)kPlans && !mbar_try(S.splan + 8u * (kPlans + q), (k / kPlans - 1u) & 1u)) return;
+            const Walk w = walk_of(jobs, njobs, u);
+            const RJob &J = jobs[w.j];
+            Plan P = {};
+            if (INTERP == 0 && J.tma_ok) {
+                if (w.j != C.last_job)  // the descriptor was written by a copy
+                    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
+                P = plan_walk<T, G>(J, w);
             }
-            const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
-            if (seq >= (uint32_t)kRing && !mbar_wait(empty, (seq / kRing - 1u) & 1u, S.abort)) { ok = false; break; }
-            if (lane == 0) mbar_expect_tx(full, slot == 0 ? 2u * bytes1 : bytes1);
             __syncwarp();
-            if (lane < P.rows) {
-                // the row warps' reads of the slot's previous plane happen
-                // before their release of it; order them before the
-                // asynchronous write
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B + (uint32_t)(lane * Gm::ROW_B);
-                const int pz = (int)(pfirst + i);
-                tma_row(d, &J.tmap, P.rx0, P.ry0 + lane, pz, full);
-                if (slot == 0) tma_row(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, P.rx0, P.ry0 + lane, pz, full);
+            if (lane == 0) {
+                S.plans[q] = P;
+                C.last_job = INTERP == 0 && J.tma_ok ? w.j : C.last_job;
+                C.j = w.j;
+                C.pfirst = w.z0 + P.a - J.src_o[2];
+                C.i = 0;
+                C.planned = 1;
             }
-            ++seq;
-            slot = slot + 1 == (uint32_t)kRing ? 0u : slot + 1;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(S.splan + 8u * q);
+            continue;
         }
-        if (!ok) break;
-        if (!more) break;
-        if (!planned) nxt = plan_of(wn);
-        u = un;
-        w = wn;
+        const Plan &P = S.plans[q];
+        const int i = C.i;
+        if (i >= P.nplanes) {  // the frontier walk is copied: on to the next
+            __syncwarp();
+            if (lane == 0) {
+                C.u = u + gridDim.x;
+                C.k = k + 1u;
+                C.planned = 0;
+            }
+            continue;
+        }
+        const uint32_t seq = C.seq, slot = C.slot;
+        const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
+        if (seq >= (uint32_t)kRing && !mbar_try(empty, (seq / kRing - 1u) & 1u)) return;
+        const RJob &J = jobs[C.j];
+        const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)P.rows;
+        const int rows = P.rows, rx0 = P.rx0, ry0 = P.ry0;
+        const int pz = (int)(C.pfirst + i);
+        __syncwarp();
+        if (lane == 0) mbar_expect_tx(full, slot == 0 ? 2u * bytes1 : bytes1);
+        __syncwarp();
+        if (lane < rows) {
+            // every warp's reads of the slot's previous plane happen before its
+            // release of it; order them before the asynchronous write
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B + (uint32_t)(lane * Gm::ROW_B);
+            tma_row(d, &J.tmap, rx0, ry0 + lane, pz, full);
+            if (slot == 0) tma_row(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, rx0, ry0 + lane, pz, full);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            C.i = i + 1;
+            C.seq = seq + 1u;
+            C.slot = slot + 1u == (uint32_t)kRing ? 0u : slot + 1u;
+        }
     }
-    // every copy issued lands before the CTA exits (bounded waits)
-    const uint32_t n0 = seq > (uint32_t)kRing ? seq - kRing : 0u;
-    for (uint32_t n = n0; n < seq; ++n)
-        if (!mbar_try(S.sfull + 8u * (n % kRing), (n / kRing) & 1u))
-            mbar_wait_slow(S.sfull + 8u * (n % kRing), (n / kRing) & 1u, S.abort, true);
-    return ok;
+}
+
+// Waits for the phase of parity `parity` of the mbarrier at `a`; warp 0
+// keeps its copier role going meanwhile.  false if the wait gave up.
+template <typename T, int G, int INTERP>
+__device__ __forceinline__ bool wait_copying(uint32_t a, uint32_t parity, bool copier, const RJob *__restrict__ jobs,
+                                             int njobs, int64_t total, const TSmem &S)
+{
+    if (mbar_try(a, parity)) return true;
+    if (!copier) return mbar_wait_slow(a, parity, S.abort, false);
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned n = 1;; ++n) {
+        copy_ahead<T, G, INTERP>(jobs, njobs, total, S);
+        if (mbar_try(a, parity)) return true;
+        if ((n & 15u) == 0 && (*reinterpret_cast<volatile int *>(S.abort) || globaltimer_ns() - t0 > kStageWaitNs))
+            return false;
+    }
 }
 
 // The row warps' state of one cell layer (uniform across the warp except
 // the position pairs).
 struct RowLayer {
     float2 P[4][3];   // per node layer c: (x, y) of voxel 0, (x, y) of voxel 1, (z0, z1)
-    Frame frame;
-    Clamp cw;
+    float mn[3], mx[3];  // the row's sample hull over the layer (frame coordinates)
     float zlo, zhi;   // a plane at frame z pz is unchecked in z when zlo <= pz < zhi
     bool row_fast;    // the row is unchecked in x and y
 };
@@ -957,22 +991,22 @@ __device__ __forceinline__ void row_layer(const RJob &J, int64_t Ox, int64_t Oy,
     // sample hull of the row over the layer's planes (frame coordinates)
     const float plo[3] = {0.f, fy, (float)zoff};
     const float phi[3] = {(float)(kTBX - 1), fy, (float)(zoff + zn - 1)};
-    float mn[3], mx[3];
+    float *mn = L.mn, *mx = L.mx;
     for (int a = 0; a < 3; ++a) {
         mn[a] = dmn[a] <= -3.0e38f ? -3.4e38f : plo[a] + dmn[a];
         mx[a] = dmx[a] >= 3.0e38f ? 3.4e38f : phi[a] + dmx[a];
     }
-    L.frame = make_frame(J, O);
-    const bool span_ok = offsets_fit_32(J, mn, mx);
-    L.cw = make_clamp(J, L.frame, mn, mx);
+    const Frame frame = make_frame(J, O);
+    const bool span_ok = offsets_fit_32(J, L.mn, L.mx);
+    const Clamp cw = make_clamp(J, frame, L.mn, L.mx);
     // unchecked-path bounds per axis: every tap of a sample q with
     // lb <= q < hb lies inside the volume and the source buffer
     float lb[3], hb[3];
     for (int a = 0; a < 3; ++a) {
-        lb[a] = fmaxf(L.frame.lo[a], (float)L.frame.bl[a]) + 1.0f / 64.0f;
-        hb[a] = fminf(L.frame.hi[a], (float)L.frame.bh[a]) - 1.0f / 64.0f;
+        lb[a] = fmaxf(frame.lo[a], (float)frame.bl[a]) + 1.0f / 64.0f;
+        hb[a] = fminf(frame.hi[a], (float)frame.bh[a]) - 1.0f / 64.0f;
     }
-    L.row_fast = span_ok && L.cw.span32 && (kTBX <= xe) && mn[0] >= lb[0] && mx[0] < hb[0] && mn[1] >= lb[1] &&
+    L.row_fast = span_ok && cw.span32 && (kTBX <= xe) && mn[0] >= lb[0] && mx[0] < hb[0] && mn[1] >= lb[1] &&
                  mx[1] < hb[1];
     L.zlo = lb[2] - dmn[2];
     L.zhi = hb[2] - dmx[2];
@@ -1072,19 +1106,19 @@ struct Gather {
 
 // A voxel pair gathered from global memory.
 template <typename T, int INTERP>
-__device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, const RowLayer &L, const Gather<T> &g,
-                                              bool fast, int nv, bool pair_ok, T *dp)
+__device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, const Frame &frame, const Clamp &cw,
+                                              const Gather<T> &g, bool fast, int nv, bool pair_ok, T *dp)
 {
     if constexpr (INTERP == 0) {
         uint32_t w;
         if (fast)
             pair_fast2<T, true>(p0, p1, pz2, g.rows, w);
-        else if (L.cw.clamped)
-            pair_clamped2<T, true>(p0, p1, pz2, g.rows, L.frame, L.cw.cl, L.cw.ch, nv, w);
-        else if (L.cw.span32)
-            pair_checked2<T, true, int>(p0, p1, pz2, g.base, g.py32, g.pz32, L.frame, L.cw.cl, L.cw.ch, nv, w);
+        else if (cw.clamped)
+            pair_clamped2<T, true>(p0, p1, pz2, g.rows, frame, cw.cl, cw.ch, nv, w);
+        else if (cw.span32)
+            pair_checked2<T, true, int>(p0, p1, pz2, g.base, g.py32, g.pz32, frame, cw.cl, cw.ch, nv, w);
         else
-            pair_checked2<T, true, int64_t>(p0, p1, pz2, g.base, g.py, g.pz, L.frame, L.cw.cl, L.cw.ch, nv, w);
+            pair_checked2<T, true, int64_t>(p0, p1, pz2, g.base, g.py, g.pz, frame, cw.cl, cw.ch, nv, w);
         store_packed<T>(dp, w, pair_ok, fast ? 2 : nv);
     } else {
         const float q[2][3] = {{p0.x, p0.y, pz2.x}, {p1.x, p1.y, pz2.y}};
@@ -1096,7 +1130,7 @@ __device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, 
                 v = sample_fast<T, INTERP>(g.base, g.py32, g.pz32, q[j][0], q[j][1], q[j][2]);
                 outv[j] = (uint32_t)v;
             } else {
-                const bool ok = j < nv && sample_checked<T, INTERP>(g.base, g.py, g.pz, L.frame, q[j][0], q[j][1],
+                const bool ok = j < nv && sample_checked<T, INTERP>(g.base, g.py, g.pz, frame, q[j][0], q[j][1],
                                                                    q[j][2], v);
                 outv[j] = ok ? (uint32_t)v : 0u;
             }
@@ -1105,13 +1139,14 @@ __device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, 
     }
 }
 
-// The row warps: every walk of the CTA, one output row per warp.  Returns
-// false if a wait gave up.
+// Every walk of the CTA, one output row per warp (warp 0 also copies).
+// Returns false if a wait gave up.
 template <typename T, int G, int INTERP>
 __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
 {
     using Gm = TGeom<T, G>;
     const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool copier = y == 0;
     const int x = 2 * lane;
     float4 *Rw = S.Rw + y * Gm::NRW;
     const float4 wx[2] = {S.W[x % G], S.W[(x + 1) % G]};
@@ -1122,11 +1157,12 @@ __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total
     for (int64_t u = blockIdx.x; u < total; u += gridDim.x, ++k) {
         const Walk w = walk_of(jobs, njobs, u);
         const RJob &J = jobs[w.j];
-        const uint32_t q = k & 1u;
-        if (!mbar_wait(S.splan + 8u * q, (k >> 1) & 1u, S.abort)) return false;
+        const uint32_t q = k % kPlans;
+        if (!wait_copying<T, G, INTERP>(S.splan + 8u * q, (k / kPlans) & 1u, copier, jobs, njobs, total, S))
+            return false;
         const Plan P = S.plans[q];
         __syncwarp();
-        if (lane == 0) mbar_arrive(S.splan + 16u + 8u * q);
+        if (lane == 0) mbar_arrive(S.splan + 8u * (kPlans + q));
         const int64_t xe64 = J.out_o[0] + J.out_n[0] - w.Ox;
         const int xe = (int)min(xe64, (int64_t)kTBX);
         const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;
@@ -1158,7 +1194,8 @@ __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total
                     // the window of plane zg: sequences (zg - z0) .. (zg - z0) + Wn - 1 of the walk
                     const uint32_t need = (uint32_t)(zg - w.z0) + (uint32_t)Wn;
                     while (waited < need) {
-                        if (!mbar_wait(S.sfull + 8u * wslot, wpar, S.abort)) return false;
+                        if (!wait_copying<T, G, INTERP>(S.sfull + 8u * wslot, wpar, copier, jobs, njobs, total, S))
+                            return false;
                         ++waited;
                         if (++wslot == (uint32_t)kRing) {
                             wslot = 0;
@@ -1173,15 +1210,18 @@ __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total
                         const uint32_t cz = rslot + (uint32_t)(int32_t)(Oz - zg - P.a) - (uint32_t)kMagicBits;
                         if (L.row_fast && pz >= L.zlo && pz < L.zhi) {
                             const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
+                            const Frame unused = {};
                             const uint32_t v =
-                                pair_staged<T, false>(sm, kxy, omax, cz, p0, p1, pz2, L.frame, wl, wh, 2);
+                                pair_staged<T, false>(sm, kxy, omax, cz, p0, p1, pz2, unused, wl, wh, 2);
                             store_packed<T>(drow + x, v, pair_ok, 2);
                         } else if (x < xe) {
+                            const int64_t O[3] = {w.Ox, w.Oy, Oz};
+                            const Frame frame = make_frame(J, O);
                             const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(zg + P.a - Oz)};
                             const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
                                                  (float)(zg + P.b - 1 - Oz)};
                             const uint32_t v =
-                                pair_staged<T, true>(sm, kxy, omax, cz, p0, p1, pz2, L.frame, wl, wh, xe - x);
+                                pair_staged<T, true>(sm, kxy, omax, cz, p0, p1, pz2, frame, wl, wh, xe - x);
                             store_packed<T>(drow + x, v, pair_ok, xe - x);
                         }
                         drow += J.dst_pz;
@@ -1190,21 +1230,26 @@ __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total
                     __syncwarp();
                     if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
                     if (++rslot == (uint32_t)kRing) rslot = 0;
+                    if (copier) copy_ahead<T, G, INTERP>(jobs, njobs, total, S);
                 }
             } else if (rowv) {
+                const int64_t O[3] = {w.Ox, w.Oy, Oz};
+                const Frame frame = make_frame(J, O);
+                const Clamp cw = make_clamp(J, frame, L.mn, L.mx);
                 Gather<T> g;
                 g.base = src + ((Oz - J.src_o[2]) * J.src_pz + (w.Oy - J.src_o[1]) * J.src_py + (w.Ox - J.src_o[0]));
                 g.py32 = (int)J.src_py;
                 g.pz32 = (int)J.src_pz;
                 g.py = J.src_py;
                 g.pz = J.src_pz;
-                g.rows = make_rows(g.base, g.py32, g.pz32, L.cw.cl, L.cw.span32);
+                g.rows = make_rows(g.base, g.py32, g.pz32, cw.cl, cw.span32);
                 for (int z = 0; z < zn; ++z) {
                     float2 p0, p1, pz2;
                     plane_positions(L, S.W[zoff + z], p0, p1, pz2);
                     const float pz = (float)(zoff + z);
                     const bool fast = L.row_fast && pz >= L.zlo && pz < L.zhi;
-                    if (fast || x < xe) gathered_pair<T, INTERP>(p0, p1, pz2, L, g, fast, xe - x, pair_ok, drow + x);
+                    if (fast || x < xe)
+                        gathered_pair<T, INTERP>(p0, p1, pz2, frame, cw, g, fast, xe - x, pair_ok, drow + x);
                     drow += J.dst_pz;
                 }
             }
@@ -1218,8 +1263,20 @@ __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total
                 if (++rslot == (uint32_t)kRing) rslot = 0;
             }
         }
+        if (copier) copy_ahead<T, G, INTERP>(jobs, njobs, total, S);
     }
     return true;
+}
+
+// Warp 0, on its way out: every copy it issued lands before the CTA exits
+// (all of them have been waited for unless a wait gave up; bounded waits).
+__device__ void drain_copies(const TSmem &S)
+{
+    const uint32_t seq = S.cs->seq;
+    const uint32_t n0 = seq > (uint32_t)kRing ? seq - kRing : 0u;
+    for (uint32_t n = n0; n < seq; ++n)
+        if (!mbar_try(S.sfull + 8u * (n % kRing), (n / kRing) & 1u))
+            mbar_wait_slow(S.sfull + 8u * (n % kRing), (n / kRing) & 1u, S.abort, true);
 }
 
 // ---------------------------------------------------------------- affine
@@ -1350,14 +1407,15 @@ __device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, 
 // ---------------------------------------------------------------- kernels
 
 template <typename T, int G, int INTERP>
-__global__ void __maxnreg__(120) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
+__global__ void __launch_bounds__(kTpsThreads, 1) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
                                                                   int64_t total_units, int *err)
 {
     using Gm = TGeom<T, G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_sh;
     // ring slots first, on a 128-byte boundary (TMA destinations), then the
-    // mbarriers, the plans, the weight table and the row warps' node rows
+    // mbarriers, the plans, the copier state, the weight table and the
+    // warps' node rows
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t pad = (128u - (raw & 127u)) & 127u;
     TSmem S;
@@ -1367,7 +1425,8 @@ __global__ void __maxnreg__(120) k_resample_tps(const RJob *__restrict__ jobs, i
     S.splan = S.sfull + 16u * kRing;
     unsigned char *tail = S.base + Gm::RING_B + 8 * Gm::NBAR;
     S.plans = reinterpret_cast<Plan *>(tail);
-    S.W = reinterpret_cast<float4 *>(tail + 2 * sizeof(Plan));
+    S.cs = reinterpret_cast<CopyState *>(tail + kPlans * sizeof(Plan));
+    S.W = reinterpret_cast<float4 *>(tail + kPlans * sizeof(Plan) + sizeof(CopyState));
     S.Rw = S.W + G;
     S.abort = &abort_sh;
     const int tid = threadIdx.x;
@@ -1376,22 +1435,27 @@ __global__ void __maxnreg__(120) k_resample_tps(const RJob *__restrict__ jobs, i
         mbar_init(S.sfull + 8u * tid, 1);
         mbar_init(S.sfull + 8u * (kRing + tid), kRowWarps);
     }
-    if (tid < 2) {
+    if (tid < kPlans) {
         mbar_init(S.splan + 8u * tid, 1);
-        mbar_init(S.splan + 16u + 8u * tid, kRowWarps);
+        mbar_init(S.splan + 8u * (kPlans + tid), kRowWarps);
     }
     if (tid == 0) {
         abort_sh = 0;
+        CopyState c = {};
+        c.u = blockIdx.x;
+        c.last_job = -1;
+        *S.cs = c;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const bool ok = (tid >> 5) == kRowWarps ? tps_copier<T, G, INTERP>(jobs, njobs, total_units, S)
-                                            : tps_rows<T, G, INTERP>(jobs, njobs, total_units, S);
+    if (tid < 32) copy_ahead<T, G, INTERP>(jobs, njobs, total_units, S);
+    const bool ok = tps_rows<T, G, INTERP>(jobs, njobs, total_units, S);
     if (!ok) {
         // the other warps see the flag in their waits and return
         *reinterpret_cast<volatile int *>(&abort_sh) = 1;
         if ((tid & 31) == 0 && err) atomicOr(err, kKernErrTimeout);
     }
+    if (tid < 32) drain_copies(S);
 }
 
 template <typename T, int INTERP>
