@@ -2,7 +2,8 @@
 
 The library is a plain C ABI (include/terawarp_b200.h); it is compiled
 directly with nvcc, not as a torch extension, so its signatures carry no
-torch types.  Output: terawarp_b200/libterawarp_b200.so.
+torch types.  Output: terawarp_b200/libterawarp_b200.so, and the command-line front end
+terawarp_b200/terawarp (cli/tw_main.cpp) linked against it.
 """
 from __future__ import annotations
 
@@ -17,6 +18,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libterawarp_b200.so"
+CLI_SRC = PKG / "cli" / "tw_main.cpp"
+CLI = PKG / "terawarp"
 BUILD = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -50,11 +53,24 @@ def _compile(src: Path, verbose: bool) -> Path:
     return obj
 
 
+def build_cli() -> Path:
+    """The terawarp executable: tw_main.cpp against the library (rpath = its own directory)."""
+    cmd = [_host_cxx(), "-O2", "-std=c++17", "-I", str(ROOT / "include"), str(CLI_SRC), "-L", str(PKG),
+           "-lterawarp_b200", "-Wl,-rpath,$ORIGIN", "-o", str(CLI) + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building the terawarp command failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(str(CLI) + ".tmp", CLI)
+    return CLI
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     srcs = sources()
     headers = list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h"))
     newest = max(p.stat().st_mtime for p in srcs + headers + [Path(__file__)])
     if OUT.exists() and not force and OUT.stat().st_mtime >= newest:
+        if not CLI.exists() or CLI.stat().st_mtime < max(OUT.stat().st_mtime, CLI_SRC.stat().st_mtime):
+            build_cli()
         return OUT
     BUILD.mkdir(exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
@@ -66,6 +82,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(str(OUT) + ".tmp", OUT)
+    build_cli()
     return OUT
 
 
