@@ -568,7 +568,7 @@ def serving_leg(ctx, device: int, n_jobs: int, seed: int = 1239, rate_hz: float 
         for j, b in zip(jobs, nbytes):
             off = 0 if off + b > ring_bytes else off
             plain(j, view(pool, 0, j, b), view(ring_pool, off, j, b))
-            off += b
+            off = (off + b + 255) & ~255  # 256-byte aligned slices (any voxel type)
         return time.perf_counter() - t0
 
     out = {"jobs": n_jobs, "rate_hz": rate_hz,

@@ -68,9 +68,14 @@ struct alignas(128) RJob {
 // jobs_dev is device memory holding the RJob array; total_bricks is the sum
 // of all jobs' bricks.  Returns a cudaError_t from the launch.
 // err: device word the kernel ORs a failure code into (a bounded wait that
-// gave up); may be null.
+// gave up); may be null.  stage_ws: for trilinear TPS, device memory of
+// tps_stage_ws_bytes(total_bricks) whose first 8 bytes are zero: the units
+// are planned, staged units run the TMA-staged kernel and the rest the
+// gather kernel; null: the gather kernel takes every unit.
 cudaError_t launch_resample(const RJob *jobs_dev, int njobs, int64_t total_bricks, int dtype,
-                            int kind, int g, int interp, cudaStream_t st, int sm_count, int *err);
+                            int kind, int g, int interp, cudaStream_t st, int sm_count, int *err,
+                            void *stage_ws);
+size_t tps_stage_ws_bytes(int64_t total_bricks);
 // Brick extents for a (kind, g) pair: x, y and the z extent a unit's frame
 // is anchored to (a control cell layer for TPS).
 void brick_dims(int kind, int g, int64_t out[3]);

@@ -63,6 +63,19 @@ RJob affine_job(const void *src, const int64_t src_sz[3], void *dst, const int64
     return j;
 }
 
+namespace {
+
+// A stream-ordered pool block returned on its stream when the scope ends.
+struct StreamBlock {
+    tw_ctx *ctx = nullptr;
+    cudaStream_t st = nullptr;
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~StreamBlock() { if (p) dfree_on(ctx, p, bytes, st); }
+};
+
+}  // namespace
+
 tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
 {
     if (njobs <= 0) return TW_OK;
@@ -89,11 +102,22 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
         count(zs);
     }
     if (total == 0) return TW_OK;
+    bool staged = false;  // some job's source can be staged by TMA
     if (jobs[0].kind == 1 && jobs[0].interp == 0)
         for (int i = 0; i < njobs; ++i) {
             if (ctx->resample_staging.load()) encode_source_map(jobs[i]);
             else jobs[i].tma_ok = 0;
+            staged = staged || jobs[i].tma_ok;
         }
+    // the units' staging plans and the list of units left to the gather kernel
+    StreamBlock fb{ctx, st};
+    if (staged) {
+        fb.bytes = tps_stage_ws_bytes(total);
+        TW_TRY(dmalloc_on(ctx, &fb.p, fb.bytes, st));
+        TW_CUDA_TRY(cudaMemsetAsync(fb.p, 0, sizeof(int64_t), st));
+    }
+    void *d_fb = fb.p;
+    const uint64_t launches = staged ? 3 : 1;
     const size_t bytes = sizeof(RJob) * (size_t)njobs;
     if (njobs <= tw_ctx::kJobsPerSlot && ctx->job_d) {
         // descriptors through the context's slot ring: an asynchronous copy
@@ -107,20 +131,20 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
         std::memcpy(h, jobs, bytes);
         TW_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
         cudaError_t e = launch_resample(d, njobs, total, jobs[0].dtype, jobs[0].kind, jobs[0].g, jobs[0].interp, st,
-                                        ctx->sm_count, ctx->d_err);
+                                        ctx->sm_count, ctx->d_err, d_fb);
         if (e != cudaSuccess) return fail(ctx, TW_ERR_CUDA, std::string("resample launch: ") + cudaGetErrorString(e));
         TW_CUDA_TRY(cudaEventRecord(ctx->job_ev[s], st));
-        count_launch(ctx);
+        count_launch(ctx, launches);
         return TW_OK;
     }
     RJob *d_jobs = nullptr;
     TW_CUDA_TRY(cudaMallocAsync((void **)&d_jobs, bytes, st));
     TW_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs, bytes, cudaMemcpyHostToDevice, st));
     cudaError_t e = launch_resample(d_jobs, njobs, total, jobs[0].dtype, jobs[0].kind, jobs[0].g, jobs[0].interp, st,
-                                    ctx->sm_count, ctx->d_err);
+                                    ctx->sm_count, ctx->d_err, d_fb);
     cudaFreeAsync(d_jobs, st);
     if (e != cudaSuccess) return fail(ctx, TW_ERR_CUDA, std::string("resample launch: ") + cudaGetErrorString(e));
-    count_launch(ctx);
+    count_launch(ctx, launches);
     return TW_OK;
 }
 

@@ -564,30 +564,30 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // hull of its nodes' displacements (B-spline weights are >= 0 and sum to 1)
 // plus the +1 tap -- is a box of at most kBoxW x kHMax elements per source
 // plane and a window of W planes that slides down one plane per output
-// plane.  Warp 0 also plans each walk, publishes the plan, and copies the
-// box's rows of every source plane the walk reads, in order, into a ring of
-// kRing plane slots by TMA (cp.async.bulk.tensor, one row per copy, from this
-// GPU's own memory; no multicast).  Each slot has a "full" mbarrier
-// (transaction count of the copies) and an "empty" mbarrier (one arrival per
-// warp once no later plane of that warp reads the slot).  Warp 0 never blocks
-// on its copier role: between its own planes, and while it waits, it issues
-// every copy whose slot has been released by all warps (and plans walks as
-// the copies reach them), so copies run up to kRing - W planes ahead of the
-// slowest warp and no warp waits for another except through the data.
+// plane.  A planning kernel (one warp per walk) computes every walk's plan
+// first and lists the walks that do not fit.  In the staged kernel warp 0
+// also copies the box's rows of every source plane its CTA's walks read, in
+// order, into a ring of kRing plane slots by TMA (cp.async.bulk.tensor, one
+// row per copy, from this GPU's own memory; no multicast).  Each slot has a
+// "full" mbarrier (transaction count of the copies) and an "empty" mbarrier
+// (one arrival per warp once no later plane of that warp reads the slot).
+// Warp 0 never blocks on its copier role: between its own planes, and while
+// it waits, it issues every copy whose slot has been released by all warps,
+// so copies run up to kRing - W planes ahead of the slowest warp and no warp
+// waits for another except through the data.
 // Slot 0 is copied a second time past the last slot,
 // so the z+1 tap of any plane is at a fixed offset.  The slots' row pitch is
 // 128 elements: a row or plane step moves an address by a multiple of 32
 // banks, so a warp's loads hit distinct banks whichever rows and planes its
 // lanes read.  A walk whose box or window does not fit, a nearest-neighbour
 // job, or a source buffer TMA cannot describe gathers from global memory
-// instead, with the same positions and the same trilinear arithmetic
-// (trilerp2).
+// instead (the gather kernel), with the same positions and the same
+// trilinear arithmetic (trilerp2).
 
 constexpr int kTBX = 64;                     // unit width (x): 32 lanes x 2 voxels
 constexpr int kTBY = 16;                     // unit height (y): one warp per row
 constexpr int kRowWarps = kTBY;
 constexpr int kTpsThreads = 32 * kRowWarps;
-constexpr int kPlans = 4;                    // plan slots: walks planned ahead of the slowest warp
 constexpr int kBoxW = kStageBoxW;            // TMA box: source elements per row copy
 constexpr int kRowP = 128;                   // shared-memory row pitch (elements)
 constexpr int kHMax = 28;                    // staged rows per plane
@@ -597,7 +597,7 @@ constexpr int kMinAhead = 2;                 // slots a walk's window leaves for
 // an error (the kernel reports kKernErrTimeout and returns)
 constexpr unsigned long long kStageWaitNs = 2000000000ull;
 
-// A walk's staging plan, written by warp 0, read by every warp.
+// A walk's staging plan (planning kernel).
 struct alignas(16) Plan {
     int staged;    // 1: the walk's source footprint is staged
     int a, b;      // output plane z reads source planes [z + a, z + b]
@@ -613,14 +613,14 @@ struct alignas(16) Plan {
 struct alignas(16) CopyState {
     int64_t u;        // flattened unit index of the frontier walk (>= total: done)
     int64_t pfirst;   // buffer z of the frontier walk's first staged plane
-    uint32_t k;       // walk number of the frontier walk (its plan slot is k % kPlans)
-    int planned;      // the frontier walk's plan is published
+    int loaded;       // the frontier walk's plan is loaded
+    int n;            // planes to copy for the frontier walk (0: not staged)
     int i;            // next plane of the frontier walk to copy
     int j;            // job of the frontier walk
+    int rows, rx0, ry0;  // the frontier walk's box
     int last_job;     // job whose tensor map was last acquired
     uint32_t seq;     // planes copied so far
     uint32_t slot;    // seq % kRing
-    int pad;
 };
 
 template <typename T, int G>
@@ -631,9 +631,9 @@ struct TGeom {
     static constexpr int ROW_B = kRowP * ES;
     static constexpr int PLANE_B = kHMax * ROW_B;
     static constexpr int RING_B = (kRing + 1) * PLANE_B;
-    static constexpr int NBAR = 2 * kRing + 2 * kPlans;  // full[kRing], empty[kRing], plan full / empty[kPlans]
-    static constexpr size_t smem_bytes = 128 + (size_t)RING_B + 8 * NBAR + kPlans * sizeof(Plan) + sizeof(CopyState) +
-                                         sizeof(float4) * (size_t)(G + kRowWarps * NRW);
+    static constexpr int NBAR = 2 * kRing;        // full[kRing], empty[kRing]
+    static constexpr size_t smem_bytes =
+        128 + (size_t)RING_B + 8 * NBAR + sizeof(CopyState) + sizeof(float4) * (size_t)(G + kRowWarps * NRW);
     static_assert((8 * NBAR) % 16 == 0 && sizeof(Plan) % 16 == 0 && sizeof(CopyState) % 16 == 0,
                   "the weight table is float4-aligned");
 };
@@ -707,8 +707,6 @@ struct TSmem {
     unsigned char *base;  // 128-byte aligned start of the ring
     uint32_t sring;       // shared-window address of slot 0
     uint32_t sfull;       // shared-window address of full[0] (8 bytes each); empty[s] = full[s] + 8 kRing
-    uint32_t splan;       // plan full[0 .. kPlans-1], then plan empty[0 .. kPlans-1]
-    Plan *plans;          // kPlans plan slots
     CopyState *cs;        // warp 0's copier state
     float4 *W;            // B-spline weights at t = i / G
     float4 *Rw;           // per row warp: y-contracted nodes of its row
@@ -748,7 +746,7 @@ __device__ __forceinline__ void warp_minmax(float (&mn)[3], float (&mx)[3])
         }
 }
 
-// Plans walk w (copy warp): the hull of the DF over the walk's node support
+// Plans walk w (one warp): the hull of the DF over the walk's node support
 // gives the staged box and the plane window.  staged = 0 when they do not
 // fit.  Every lane returns the same plan.
 template <typename T, int G>
@@ -812,54 +810,50 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     return P;
 }
 
-// Warp 0's copier role, never blocking: plans and publishes walks and
-// issues plane copies, in ring order, for as long as plan slots and ring
-// slots are free (released by every warp).  Called by warp 0 between its
-// planes and while it waits.
-template <typename T, int G, int INTERP>
-__device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
+// Warp 0's copier role, never blocking: issues plane copies of the CTA's
+// staged walks (plans from the planning kernel), in ring order, for as long
+// as ring slots are free (released by every warp).  Called by warp 0 between
+// its planes and while it waits.
+template <typename T, int G>
+__device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t total, const Plan *__restrict__ plans,
+                           const TSmem &S)
 {
     using Gm = TGeom<T, G>;
     const int lane = threadIdx.x & 31;
     CopyState &C = *S.cs;
     // bounded work per call: a ring's worth of copies and a few walks
-    for (int step = 0; step < kRing + 2 * kPlans; ++step) {
+    for (int step = 0; step < kRing + 8; ++step) {
         __syncwarp();  // lane 0's last update of C is visible
         const int64_t u = C.u;
         if (u >= total) return;
-        const uint32_t k = C.k, q = k % kPlans;
-        if (!C.planned) {
-            // the plan slot is free once every warp has read the plan kPlans walks back
-            if (k >= (uint32_t)kPlans && !mbar_try(S.splan + 8u * (kPlans + q), (k / kPlans - 1u) & 1u)) return;
-            const Walk w = walk_of(jobs, njobs, u);
-            const RJob &J = jobs[w.j];
-            Plan P = {};
-            if (INTERP == 0 && J.tma_ok) {
-                if (w.j != C.last_job)  // the descriptor was written by a copy
-                    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
-                P = plan_walk<T, G>(J, w);
-            }
+        if (!C.loaded) {
+            const Plan P = plans[u];
+            const int j = find_job(jobs, njobs, u);
+            const RJob &J = jobs[j];
+            const int64_t lu = u - J.brick_begin;
+            const int64_t z0 = J.out_o[2] + (lu / (J.bricks[0] * J.bricks[1])) * J.zs;
+            if (P.staged && j != C.last_job)  // the descriptor was written by a copy
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
             __syncwarp();
             if (lane == 0) {
-                S.plans[q] = P;
-                C.last_job = INTERP == 0 && J.tma_ok ? w.j : C.last_job;
-                C.j = w.j;
-                C.pfirst = w.z0 + P.a - J.src_o[2];
+                C.n = P.staged ? P.nplanes : 0;
                 C.i = 0;
-                C.planned = 1;
+                C.j = j;
+                C.rows = P.rows;
+                C.rx0 = P.rx0;
+                C.ry0 = P.ry0;
+                C.pfirst = z0 + P.a - J.src_o[2];
+                if (P.staged) C.last_job = j;
+                C.loaded = 1;
             }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(S.splan + 8u * q);
             continue;
         }
-        const Plan &P = S.plans[q];
         const int i = C.i;
-        if (i >= P.nplanes) {  // the frontier walk is copied: on to the next
+        if (i >= C.n) {  // the frontier walk is copied: on to the next
             __syncwarp();
             if (lane == 0) {
                 C.u = u + gridDim.x;
-                C.k = k + 1u;
-                C.planned = 0;
+                C.loaded = 0;
             }
             continue;
         }
@@ -867,8 +861,8 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
         const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
         if (seq >= (uint32_t)kRing && !mbar_try(empty, (seq / kRing - 1u) & 1u)) return;
         const RJob &J = jobs[C.j];
-        const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)P.rows;
-        const int rows = P.rows, rx0 = P.rx0, ry0 = P.ry0;
+        const int rows = C.rows, rx0 = C.rx0, ry0 = C.ry0;
+        const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)rows;
         const int pz = (int)(C.pfirst + i);
         __syncwarp();
         if (lane == 0) mbar_expect_tx(full, slot == 0 ? 2u * bytes1 : bytes1);
@@ -892,15 +886,15 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
 
 // Waits for the phase of parity `parity` of the mbarrier at `a`; warp 0
 // keeps its copier role going meanwhile.  false if the wait gave up.
-template <typename T, int G, int INTERP>
+template <typename T, int G>
 __device__ __forceinline__ bool wait_copying(uint32_t a, uint32_t parity, bool copier, const RJob *__restrict__ jobs,
-                                             int njobs, int64_t total, const TSmem &S)
+                                             int njobs, int64_t total, const Plan *__restrict__ plans, const TSmem &S)
 {
     if (mbar_try(a, parity)) return true;
     if (!copier) return mbar_wait_slow(a, parity, S.abort, false);
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned n = 1;; ++n) {
-        copy_ahead<T, G, INTERP>(jobs, njobs, total, S);
+        copy_ahead<T, G>(jobs, njobs, total, plans, S);
         if (mbar_try(a, parity)) return true;
         if ((n & 15u) == 0 && (*reinterpret_cast<volatile int *>(S.abort) || globaltimer_ns() - t0 > kStageWaitNs))
             return false;
@@ -1139,10 +1133,12 @@ __device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, 
     }
 }
 
-// Every walk of the CTA, one output row per warp (warp 0 also copies).
-// Returns false if a wait gave up.
-template <typename T, int G, int INTERP>
-__device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total, const TSmem &S)
+// The staged kernel's warps: every walk of the CTA, one output row per warp
+// (warp 0 also copies); walks that could not be planned are skipped (the
+// gather kernel takes them).  Returns false if a wait gave up.
+template <typename T, int G>
+__device__ bool rows_staged(const RJob *__restrict__ jobs, int njobs, int64_t total, const Plan *__restrict__ plans,
+                            const TSmem &S)
 {
     using Gm = TGeom<T, G>;
     const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1153,119 +1149,125 @@ __device__ bool tps_rows(const RJob *__restrict__ jobs, int njobs, int64_t total
     const unsigned char *sm = S.base;
     uint32_t wslot = 0, wpar = 0;  // next ring sequence to wait for: slot, phase parity
     uint32_t rslot = 0;            // slot of the next sequence to release
-    uint32_t k = 0;
-    for (int64_t u = blockIdx.x; u < total; u += gridDim.x, ++k) {
+    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+        const Plan P = plans[u];
+        if (!P.staged) continue;
         const Walk w = walk_of(jobs, njobs, u);
         const RJob &J = jobs[w.j];
-        const uint32_t q = k % kPlans;
-        if (!wait_copying<T, G, INTERP>(S.splan + 8u * q, (k / kPlans) & 1u, copier, jobs, njobs, total, S))
-            return false;
-        const Plan P = S.plans[q];
-        __syncwarp();
-        if (lane == 0) mbar_arrive(S.splan + 8u * (kPlans + q));
-        const int64_t xe64 = J.out_o[0] + J.out_n[0] - w.Ox;
-        const int xe = (int)min(xe64, (int64_t)kTBX);
+        const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
         const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;
-        const T *src = static_cast<const T *>(J.src);
-        T *dst = static_cast<T *>(J.dst);
+        const int64_t dst_pz = J.dst_pz;
         // a voxel pair (even x) can be written as one 2-element store
         const bool pair_ok =
             (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
-        const int Wn = P.b - P.a + 1;  // planes of a staged window
-        uint32_t waited = 0;           // sequences of this walk waited for
+        T *drow = static_cast<T *>(J.dst) +
+                  ((w.z0 - J.out_o[2]) * dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
+        // frame (0, 0) in slot 0 minus the magic-float bias of the floor bit
+        // patterns (2^32 wrap arithmetic)
+        const uint32_t kxy =
+            (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
+        const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
+        const int Wn = P.b - P.a + 1;  // planes of a window
+        int waited = 0, need = Wn;     // sequences of this walk waited for / needed by the next plane
         for (int64_t zf = w.z0; zf < w.z1;) {
             const int64_t ze = min(w.z1, (zf / G + 1) * G);
             const int64_t Oz = (zf / G) * G;
             const int zoff = (int)(zf - Oz), zn = (int)(ze - zf);
             RowLayer L;
-            T *drow = nullptr;
-            if (rowv) {
-                row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, S.W, Rw, wx, L);
-                drow = dst + ((zf - J.out_o[2]) * J.dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
-            }
-            if (INTERP == 0 && P.staged) {
-                // frame (0, 0) in slot 0 minus the magic-float bias of the
-                // floor bit patterns (2^32 wrap arithmetic)
-                const uint32_t kxy = (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B +
-                                     (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
-                const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
-                for (int z = 0; z < zn; ++z) {
-                    const int64_t zg = zf + z;
-                    // the window of plane zg: sequences (zg - z0) .. (zg - z0) + Wn - 1 of the walk
-                    const uint32_t need = (uint32_t)(zg - w.z0) + (uint32_t)Wn;
-                    while (waited < need) {
-                        if (!wait_copying<T, G, INTERP>(S.sfull + 8u * wslot, wpar, copier, jobs, njobs, total, S))
-                            return false;
-                        ++waited;
-                        if (++wslot == (uint32_t)kRing) {
-                            wslot = 0;
-                            wpar ^= 1u;
-                        }
+            if (rowv) row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, S.W, Rw, wx, L);
+            for (int pz = zoff; pz < zoff + zn; ++pz) {  // frame z of the plane
+                while (waited < need) {
+                    if (!wait_copying<T, G>(S.sfull + 8u * wslot, wpar, copier, jobs, njobs, total, plans, S))
+                        return false;
+                    ++waited;
+                    if (++wslot == (uint32_t)kRing) {
+                        wslot = 0;
+                        wpar ^= 1u;
                     }
-                    if (rowv) {
-                        float2 p0, p1, pz2;
-                        plane_positions(L, S.W[zoff + z], p0, p1, pz2);
-                        const float pz = (float)(zoff + z);
-                        // slot of a tap plane: t = (plane - window start) + slot(window start)
-                        const uint32_t cz = rslot + (uint32_t)(int32_t)(Oz - zg - P.a) - (uint32_t)kMagicBits;
-                        if (L.row_fast && pz >= L.zlo && pz < L.zhi) {
-                            const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
-                            const Frame unused = {};
-                            const uint32_t v =
-                                pair_staged<T, false>(sm, kxy, omax, cz, p0, p1, pz2, unused, wl, wh, 2);
-                            store_packed<T>(drow + x, v, pair_ok, 2);
-                        } else if (x < xe) {
-                            const int64_t O[3] = {w.Ox, w.Oy, Oz};
-                            const Frame frame = make_frame(J, O);
-                            const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(zg + P.a - Oz)};
-                            const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
-                                                 (float)(zg + P.b - 1 - Oz)};
-                            const uint32_t v =
-                                pair_staged<T, true>(sm, kxy, omax, cz, p0, p1, pz2, frame, wl, wh, xe - x);
-                            store_packed<T>(drow + x, v, pair_ok, xe - x);
-                        }
-                        drow += J.dst_pz;
-                    }
-                    // the window start is not read by later planes
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
-                    if (++rslot == (uint32_t)kRing) rslot = 0;
-                    if (copier) copy_ahead<T, G, INTERP>(jobs, njobs, total, S);
                 }
-            } else if (rowv) {
-                const int64_t O[3] = {w.Ox, w.Oy, Oz};
-                const Frame frame = make_frame(J, O);
-                const Clamp cw = make_clamp(J, frame, L.mn, L.mx);
-                Gather<T> g;
-                g.base = src + ((Oz - J.src_o[2]) * J.src_pz + (w.Oy - J.src_o[1]) * J.src_py + (w.Ox - J.src_o[0]));
-                g.py32 = (int)J.src_py;
-                g.pz32 = (int)J.src_pz;
-                g.py = J.src_py;
-                g.pz = J.src_pz;
-                g.rows = make_rows(g.base, g.py32, g.pz32, cw.cl, cw.span32);
-                for (int z = 0; z < zn; ++z) {
+                if (rowv) {
                     float2 p0, p1, pz2;
-                    plane_positions(L, S.W[zoff + z], p0, p1, pz2);
-                    const float pz = (float)(zoff + z);
-                    const bool fast = L.row_fast && pz >= L.zlo && pz < L.zhi;
-                    if (fast || x < xe)
-                        gathered_pair<T, INTERP>(p0, p1, pz2, frame, cw, g, fast, xe - x, pair_ok, drow + x);
-                    drow += J.dst_pz;
+                    plane_positions(L, S.W[pz], p0, p1, pz2);
+                    const float fz = (float)pz;
+                    // slot of a tap plane: (tap plane - window start) + slot(window start)
+                    const uint32_t cz = rslot - (uint32_t)(pz + P.a) - (uint32_t)kMagicBits;
+                    if (L.row_fast && fz >= L.zlo && fz < L.zhi) {
+                        const Frame unused = {};
+                        const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
+                        const uint32_t v = pair_staged<T, false>(sm, kxy, omax, cz, p0, p1, pz2, unused, wl, wh, 2);
+                        store_packed<T>(drow + x, v, pair_ok, 2);
+                    } else if (x < xe) {
+                        const int64_t O[3] = {w.Ox, w.Oy, Oz};
+                        const Frame frame = make_frame(J, O);
+                        const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(pz + P.a)};
+                        const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
+                                             (float)(pz + P.b - 1)};
+                        const uint32_t v = pair_staged<T, true>(sm, kxy, omax, cz, p0, p1, pz2, frame, wl, wh, xe - x);
+                        store_packed<T>(drow + x, v, pair_ok, xe - x);
+                    }
                 }
+                drow += dst_pz;
+                // the window start is not read by later planes
+                __syncwarp();
+                if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
+                if (++rslot == (uint32_t)kRing) rslot = 0;
+                ++need;
+                if (copier) copy_ahead<T, G>(jobs, njobs, total, plans, S);
             }
             zf = ze;
         }
-        if (INTERP == 0 && P.staged) {
-            // the rest of the last window
-            __syncwarp();
-            for (int i = 1; i < Wn; ++i) {
-                if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
-                if (++rslot == (uint32_t)kRing) rslot = 0;
-            }
+        // the rest of the last window
+        __syncwarp();
+        for (int i = 1; i < Wn; ++i) {
+            if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
+            if (++rslot == (uint32_t)kRing) rslot = 0;
         }
-        if (copier) copy_ahead<T, G, INTERP>(jobs, njobs, total, S);
     }
     return true;
+}
+
+// One unit gathered from global memory (gather kernel): warp y computes
+// output row y of the unit at flattened index u.
+template <typename T, int G, int INTERP>
+__device__ void rows_gather(const RJob *__restrict__ jobs, int njobs, int64_t u, const float4 *W, float4 *Rw,
+                            const float4 (&wx)[2])
+{
+    const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int x = 2 * lane;
+    const Walk w = walk_of(jobs, njobs, u);
+    const RJob &J = jobs[w.j];
+    const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
+    if ((int64_t)y >= J.out_o[1] + J.out_n[1] - w.Oy) return;
+    const T *src = static_cast<const T *>(J.src);
+    const bool pair_ok = (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
+    T *drow = static_cast<T *>(J.dst) +
+              ((w.z0 - J.out_o[2]) * J.dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
+    for (int64_t zf = w.z0; zf < w.z1;) {
+        const int64_t ze = min(w.z1, (zf / G + 1) * G);
+        const int64_t Oz = (zf / G) * G;
+        const int zoff = (int)(zf - Oz), zn = (int)(ze - zf);
+        RowLayer L;
+        row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, W, Rw, wx, L);
+        const int64_t O[3] = {w.Ox, w.Oy, Oz};
+        const Frame frame = make_frame(J, O);
+        const Clamp cw = make_clamp(J, frame, L.mn, L.mx);
+        Gather<T> g;
+        g.base = src + ((Oz - J.src_o[2]) * J.src_pz + (w.Oy - J.src_o[1]) * J.src_py + (w.Ox - J.src_o[0]));
+        g.py32 = (int)J.src_py;
+        g.pz32 = (int)J.src_pz;
+        g.py = J.src_py;
+        g.pz = J.src_pz;
+        g.rows = make_rows(g.base, g.py32, g.pz32, cw.cl, cw.span32);
+        for (int pz = zoff; pz < zoff + zn; ++pz) {
+            float2 p0, p1, pz2;
+            plane_positions(L, W[pz], p0, p1, pz2);
+            const float fz = (float)pz;
+            const bool fast = L.row_fast && fz >= L.zlo && fz < L.zhi;
+            if (fast || x < xe) gathered_pair<T, INTERP>(p0, p1, pz2, frame, cw, g, fast, xe - x, pair_ok, drow + x);
+            drow += J.dst_pz;
+        }
+        zf = ze;
+    }
 }
 
 // Warp 0, on its way out: every copy it issued lands before the CTA exits
@@ -1406,27 +1408,50 @@ __device__ void affine_brick(const RJob &J, int64_t bx, int64_t by, int64_t bz, 
 
 // ---------------------------------------------------------------- kernels
 
-template <typename T, int G, int INTERP>
-__global__ void __launch_bounds__(kTpsThreads, 1) k_resample_tps(const RJob *__restrict__ jobs, int njobs,
-                                                                  int64_t total_units, int *err)
+// Plans every unit (one warp each, 8 per CTA): plans[u], and the units that
+// cannot be staged appended to fb ([0] count, then unit indices).
+template <typename T, int G>
+__global__ void __launch_bounds__(256) k_tps_plan(const RJob *__restrict__ jobs, int njobs, int64_t total_units,
+                                                  Plan *__restrict__ plans, int64_t *fb)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t)gridDim.x * 8;
+    for (int64_t u = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5); u < total_units; u += nw) {
+        const Walk w = walk_of(jobs, njobs, u);
+        const RJob &J = jobs[w.j];
+        Plan P = {};
+        if (J.tma_ok) P = plan_walk<T, G>(J, w);
+        if (lane == 0) {
+            plans[u] = P;
+            if (!P.staged) {
+                const unsigned long long n = atomicAdd(reinterpret_cast<unsigned long long *>(fb), 1ull);
+                fb[1 + n] = u;
+            }
+        }
+    }
+}
+
+// TPS units whose source footprint is staged by TMA (trilinear), with the
+// plans of k_tps_plan; units without a staged plan are left to k_tps_gather.
+template <typename T, int G>
+__global__ void __launch_bounds__(kTpsThreads, 1) k_tps_staged(const RJob *__restrict__ jobs, int njobs,
+                                                                int64_t total_units, const Plan *__restrict__ plans,
+                                                                int *err)
 {
     using Gm = TGeom<T, G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_sh;
     // ring slots first, on a 128-byte boundary (TMA destinations), then the
-    // mbarriers, the plans, the copier state, the weight table and the
-    // warps' node rows
+    // mbarriers, the copier state, the weight table and the warps' node rows
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t pad = (128u - (raw & 127u)) & 127u;
     TSmem S;
     S.base = smem_raw + pad;
     S.sring = raw + pad;
     S.sfull = S.sring + (uint32_t)Gm::RING_B;
-    S.splan = S.sfull + 16u * kRing;
     unsigned char *tail = S.base + Gm::RING_B + 8 * Gm::NBAR;
-    S.plans = reinterpret_cast<Plan *>(tail);
-    S.cs = reinterpret_cast<CopyState *>(tail + kPlans * sizeof(Plan));
-    S.W = reinterpret_cast<float4 *>(tail + kPlans * sizeof(Plan) + sizeof(CopyState));
+    S.cs = reinterpret_cast<CopyState *>(tail);
+    S.W = reinterpret_cast<float4 *>(tail + sizeof(CopyState));
     S.Rw = S.W + G;
     S.abort = &abort_sh;
     const int tid = threadIdx.x;
@@ -1434,10 +1459,6 @@ __global__ void __launch_bounds__(kTpsThreads, 1) k_resample_tps(const RJob *__r
     if (tid < kRing) {
         mbar_init(S.sfull + 8u * tid, 1);
         mbar_init(S.sfull + 8u * (kRing + tid), kRowWarps);
-    }
-    if (tid < kPlans) {
-        mbar_init(S.splan + 8u * tid, 1);
-        mbar_init(S.splan + 8u * (kPlans + tid), kRowWarps);
     }
     if (tid == 0) {
         abort_sh = 0;
@@ -1448,14 +1469,34 @@ __global__ void __launch_bounds__(kTpsThreads, 1) k_resample_tps(const RJob *__r
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid < 32) copy_ahead<T, G, INTERP>(jobs, njobs, total_units, S);
-    const bool ok = tps_rows<T, G, INTERP>(jobs, njobs, total_units, S);
+    if (tid < 32) copy_ahead<T, G>(jobs, njobs, total_units, plans, S);
+    const bool ok = rows_staged<T, G>(jobs, njobs, total_units, plans, S);
     if (!ok) {
         // the other warps see the flag in their waits and return
         *reinterpret_cast<volatile int *>(&abort_sh) = 1;
         if ((tid & 31) == 0 && err) atomicOr(err, kKernErrTimeout);
     }
     if (tid < 32) drain_copies(S);
+}
+
+// TPS units gathered from global memory: the units of fb when it is given
+// (the staged kernel's fallback list), else units [0, total_units).
+template <typename T, int G, int INTERP>
+__global__ void __launch_bounds__(kTpsThreads, 1) k_tps_gather(const RJob *__restrict__ jobs, int njobs,
+                                                                int64_t total_units, const int64_t *fb)
+{
+    using Gm = TGeom<T, G>;
+    __shared__ float4 W[G];
+    __shared__ float4 Rw[kRowWarps * Gm::NRW];
+    const int tid = threadIdx.x;
+    if (tid < G) W[tid] = bspline_w(tid, G);
+    __syncthreads();
+    const int x = 2 * (tid & 31);
+    const float4 wx[2] = {W[x % G], W[(x + 1) % G]};
+    float4 *rw = Rw + (tid >> 5) * Gm::NRW;
+    const int64_t n = fb ? fb[0] : total_units;
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x)
+        rows_gather<T, G, INTERP>(jobs, njobs, fb ? fb[1 + i] : i, W, rw, wx);
 }
 
 template <typename T, int INTERP>
@@ -1475,21 +1516,47 @@ __global__ void __launch_bounds__(kThreads) k_resample_affine(const RJob *__rest
     }
 }
 
+// TPS launches: trilinear jobs run the planning kernel, the staged kernel
+// and the gather kernel over the planning kernel's fallback list (ws: the
+// list, 1 + total int64 with the count zeroed by the caller, then the plans
+// on a 16-byte boundary); nearest-neighbour jobs, or a launch without ws, run
+// the gather kernel over every unit.
 template <typename T, int G, int INTERP>
-cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_t st, int sms, int *err)
+cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_t st, int sms, int *err, void *ws)
 {
     using Gm = TGeom<T, G>;
-    auto k = k_resample_tps<T, G, INTERP>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
-    if (e != cudaSuccess) return e;
+    int64_t *fb = static_cast<int64_t *>(ws);
+    if (INTERP == 0 && fb) {
+        Plan *plans = reinterpret_cast<Plan *>(fb + ((1 + total + 1) & ~(int64_t)1));
+        int64_t pgrid = (total + 7) / 8;
+        if (pgrid > (int64_t)sms * 8) pgrid = (int64_t)sms * 8;
+        k_tps_plan<T, G><<<(unsigned)pgrid, 256, 0, st>>>(jobs, njobs, total, plans, fb);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        auto k = k_tps_staged<T, G>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTpsThreads, Gm::smem_bytes);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        int64_t grid = (int64_t)sms * per_sm;
+        if (grid > total) grid = total;
+        if (grid < 1) grid = 1;
+        k<<<(unsigned)grid, kTpsThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, plans, err);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    auto kg = k_tps_gather<T, G, INTERP>;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTpsThreads, Gm::smem_bytes);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kg, kTpsThreads, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int64_t grid = (int64_t)sms * per_sm;
-    if (grid > total) grid = total;
+    const bool listed = INTERP == 0 && fb;
+    if (!listed && grid > total) grid = total;
     if (grid < 1) grid = 1;
-    k<<<(unsigned)grid, kTpsThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, err);
+    kg<<<(unsigned)grid, kTpsThreads, 0, st>>>(jobs, njobs, total, listed ? fb : nullptr);
     return cudaGetLastError();
 }
 
@@ -1509,19 +1576,25 @@ cudaError_t launch_affine_t(const RJob *jobs, int njobs, int64_t total, cudaStre
 }
 
 template <typename T, int INTERP>
-cudaError_t dispatch_g(const RJob *jobs, int njobs, int64_t total, int g, cudaStream_t st, int sms, int *err)
+cudaError_t dispatch_g(const RJob *jobs, int njobs, int64_t total, int g, cudaStream_t st, int sms, int *err,
+                       void *fb)
 {
     switch (g) {
-    case 4: return launch_tps_t<T, 4, INTERP>(jobs, njobs, total, st, sms, err);
-    case 8: return launch_tps_t<T, 8, INTERP>(jobs, njobs, total, st, sms, err);
-    case 16: return launch_tps_t<T, 16, INTERP>(jobs, njobs, total, st, sms, err);
-    case 32: return launch_tps_t<T, 32, INTERP>(jobs, njobs, total, st, sms, err);
-    case 64: return launch_tps_t<T, 64, INTERP>(jobs, njobs, total, st, sms, err);
+    case 4: return launch_tps_t<T, 4, INTERP>(jobs, njobs, total, st, sms, err, fb);
+    case 8: return launch_tps_t<T, 8, INTERP>(jobs, njobs, total, st, sms, err, fb);
+    case 16: return launch_tps_t<T, 16, INTERP>(jobs, njobs, total, st, sms, err, fb);
+    case 32: return launch_tps_t<T, 32, INTERP>(jobs, njobs, total, st, sms, err, fb);
+    case 64: return launch_tps_t<T, 64, INTERP>(jobs, njobs, total, st, sms, err, fb);
     default: return cudaErrorInvalidValue;
     }
 }
 
 }  // namespace
+
+size_t tps_stage_ws_bytes(int64_t total_bricks)
+{
+    return sizeof(int64_t) * (size_t)((1 + total_bricks + 1) & ~(int64_t)1) + sizeof(Plan) * (size_t)total_bricks;
+}
 
 bool g_supported(int g) { return g == 4 || g == 8 || g == 16 || g == 32 || g == 64; }
 
@@ -1537,7 +1610,7 @@ void brick_dims(int kind, int g, int64_t out[3])
 }
 
 cudaError_t launch_resample(const RJob *jobs_dev, int njobs, int64_t total_bricks, int dtype, int kind, int g,
-                            int interp, cudaStream_t st, int sm_count, int *err)
+                            int interp, cudaStream_t st, int sm_count, int *err, void *stage_ws)
 {
     if (total_bricks <= 0) return cudaSuccess;
     if (kind == 0) {
@@ -1546,10 +1619,11 @@ cudaError_t launch_resample(const RJob *jobs_dev, int njobs, int64_t total_brick
         return interp ? launch_affine_t<uint16_t, 1>(jobs_dev, njobs, total_bricks, st, sm_count)
                       : launch_affine_t<uint16_t, 0>(jobs_dev, njobs, total_bricks, st, sm_count);
     }
-    if (dtype == 1) return interp ? dispatch_g<uint8_t, 1>(jobs_dev, njobs, total_bricks, g, st, sm_count, err)
-                                  : dispatch_g<uint8_t, 0>(jobs_dev, njobs, total_bricks, g, st, sm_count, err);
-    return interp ? dispatch_g<uint16_t, 1>(jobs_dev, njobs, total_bricks, g, st, sm_count, err)
-                  : dispatch_g<uint16_t, 0>(jobs_dev, njobs, total_bricks, g, st, sm_count, err);
+    if (dtype == 1)
+        return interp ? dispatch_g<uint8_t, 1>(jobs_dev, njobs, total_bricks, g, st, sm_count, err, nullptr)
+                      : dispatch_g<uint8_t, 0>(jobs_dev, njobs, total_bricks, g, st, sm_count, err, stage_ws);
+    return interp ? dispatch_g<uint16_t, 1>(jobs_dev, njobs, total_bricks, g, st, sm_count, err, nullptr)
+                  : dispatch_g<uint16_t, 0>(jobs_dev, njobs, total_bricks, g, st, sm_count, err, stage_ws);
 }
 
 }  // namespace tw
