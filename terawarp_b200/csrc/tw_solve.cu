@@ -326,60 +326,83 @@ __device__ __forceinline__ void signal_done(int *flag, int value)
     }
 }
 
-// potrf of diagonal block kb in shared memory: in step j threads j..63 take
-// the pivot (x rsqrt(d)) and scale column j, then each thread updates its 4 x 4
-// patch of the trailing lower triangle from register copies of the column.
+// potrf of diagonal block kb: thread t holds its 4 x 4 patch (rows tr + 16u,
+// columns tc + 16v) of the block in registers.  In step j the pivot's owner
+// publishes it; the owners of column j scale their elements of it (x
+// rsqrt(pivot)) and publish them; every thread then updates its patch of the
+// trailing lower triangle from the published column.  Two CTA barriers per
+// column and no shared-memory read-modify-write.
 __device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, double *sm)
 {
-    double(*a)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
-    double *sd = sm + kNB * (kNB + 1);
+    double *col = sm;        // column j, scaled
+    double *piv = sm + kNB;  // pivot of column j
     const int r0 = kb * kNB;
     const int nb = min(kNB, m - r0);
-    __syncthreads();
-#pragma unroll 4
-    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-        int r = e / kNB, c = e % kNB;
-        a[r][c] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
-    }
-    __syncthreads();
     const int t = threadIdx.x;
-    // thread t updates rows tr + 16u and columns tc + 16v of the block: the
-    // 16 threads of a half-warp then read 16 consecutive rows of a column
-    // (distinct banks with the 65-double row pitch)
     const int tr = t >> 4, tc = t & 15;
+    double a[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = tr + 16 * u, c = tc + 16 * v;
+            a[u][v] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
+        }
+    __syncthreads();  // sm is free (the caller's previous task may still read it)
+#pragma unroll 1
     for (int j = 0; j < kNB; ++j) {
-        if (t >= j && t < kNB) {
-            double d = a[j][j];
-            if (!(d > 0.0)) {
-                if (t == j) atomicOr(status, kStNotSPD);
-                d = 1.0;
-            }
-            const double inv = rsqrt(d);
-            if (t == j) sd[j] = d * inv;
-            else a[t][j] *= inv;
+        const int uj = j >> 4, cj = j & 15;
+        // the pivot's owner: row j, column j
+        if (tr == cj && tc == cj) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (u == uj) piv[0] = a[u][u];
         }
         __syncthreads();
-        if (tr + 48 > j) {
-            double ci[4], cl[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                ci[u] = a[tr + 16 * u][j];
-                cl[u] = a[tc + 16 * u][j];
-            }
+        double d = piv[0];
+        if (!(d > 0.0)) {
+            if (t == 0) atomicOr(status, kStNotSPD);
+            d = 1.0;
+        }
+        const double inv = rsqrt(d);
+        if (tc == cj) {
+            // this thread owns column j at rows tr + 16u
 #pragma unroll
             for (int u = 0; u < 4; ++u)
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const int i = tr + 16 * u, l = tc + 16 * v;
-                    if (l > j && i >= l) a[i][l] -= ci[u] * cl[v];
-                }
+                for (int v = 0; v < 4; ++v)
+                    if (v == uj) {
+                        const int i = tr + 16 * u;
+                        if (i > j) {
+                            a[u][v] *= inv;
+                            col[i] = a[u][v];
+                        } else if (i == j) {
+                            a[u][v] = d * inv;
+                        }
+                    }
         }
         __syncthreads();
+        double ci[4], cl[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            ci[u] = col[tr + 16 * u];
+            cl[u] = col[tc + 16 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int i = tr + 16 * u, l = tc + 16 * v;
+                if (l > j && i >= l) a[u][v] -= ci[u] * cl[v];
+            }
     }
-    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-        int r = e / kNB, c = e % kNB;
-        if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c < r ? a[r][c] : (c == r ? sd[r] : 0.0);
-    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = tr + 16 * u, c = tc + 16 * v;
+            if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c <= r ? a[u][v] : 0.0;
+        }
 }
 
 // trsm of row block ib against diagonal block kb: L(ib,kb) = A(ib,kb) L(kb,kb)^-T.
