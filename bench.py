@@ -34,6 +34,7 @@ replica (the path needs no collective); value = all ranks' voxels / max time.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import datetime
 import json
 import os
@@ -71,6 +72,8 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=1000, help="jobs in the serving leg")
     ap.add_argument("--small", action="store_true", help="256x256x128 case, 64 landmarks")
     ap.add_argument("--shape", type=str, default="", help="X,Y,Z volume for profiling captures (default: full)")
+    ap.add_argument("--resample", choices=["staged", "gather"], default="staged",
+                    help="TPS resample path: TMA-staged source footprint, or gathers from global memory")
     return ap.parse_args()
 
 
@@ -676,6 +679,10 @@ def run_ours(args):
     dst = torch.empty_like(src)
     sub, tar = case.marker_sub, case.marker_tar
     ctx = tw.Context(local)
+    if args.resample == "gather":
+        set_staging = ctx.lib.tw_internal_set_resample_staging
+        set_staging.restype, set_staging.argtypes = C.c_int, [C.c_void_p, C.c_int]
+        set_staging(ctx.handle, 0)
     gsz = (tw.grid_size(X, G), tw.grid_size(Y, G), tw.grid_size(Z, G))
     nodes = torch.empty((gsz[2], gsz[1], gsz[0], 4), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
@@ -748,7 +755,8 @@ def run_ours(args):
                    "volume_xyz": [X, Y, Z], "landmarks": n, "grid_spacing": G, "interp": "trilinear",
                    "parallelism": f"replicas x{ws}", "l2": "input 8 GiB > 126 MB L2 (no flush needed)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "kernel": "k_resample_tps<uint16,16>",
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": ("k_tps_plan + k_tps_staged + k_tps_gather<uint16,16>" if args.resample == "staged"
+                                else "k_tps_gather<uint16,16>"),
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": warp_avg},
         "gpu_launches": launches,
         "clocks": clocks,

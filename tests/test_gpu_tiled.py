@@ -127,11 +127,23 @@ def test_edge_tiles_are_batched_and_equal_the_whole_volume(ctx, case):
     t = tw.tps_solve(ctx, tar, sub)
     solve_launches = ctx.kernel_launches - n0
     t.close()
+    # kernel launches of one resample pass (planning + staged + gather kernels
+    # for a stageable trilinear job) on a small device volume of the same kind
+    t = tw.tps_solve(ctx, tar, sub)
+    small = torch.from_numpy(np.ascontiguousarray(img[:16, :64, :128])).cuda()
+    nodes = tw.tps_eval_grid(ctx, t, (tw.grid_size(128, 8), tw.grid_size(64, 8), tw.grid_size(16, 8)), 8)
+    out = torch.empty_like(small)
+    n1 = ctx.kernel_launches
+    tw.warp_tps_device(ctx, nodes, 8, small, out)
+    per_pass = ctx.kernel_launches - n1
+    t.close()
     before = ctx.kernel_launches
     tiled = api.imgwarp_smallmemory_tiled(ctx, sub, tar, 1.0, 8, img, tile=(256, 128, 64), depth=2)
     resample_launches = ctx.kernel_launches - before - solve_launches - 2  # node grid + tile hulls
+    assert resample_launches % per_pass == 0
+    passes = resample_launches // per_pass
     # tiles: x 256, 256, 8; y 128, 128, 44; z 64, 32 -> 18 tiles, 4 of them full
     ntiles, nfull = 18, 4
-    assert resample_launches < ntiles
-    assert resample_launches >= nfull + 1
+    assert passes < ntiles
+    assert passes >= nfull + 1
     np.testing.assert_array_equal(tiled, whole)
