@@ -673,6 +673,22 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
     return ok != 0;
 }
 
+// Has the phase of parity `parity` of the mbarrier at `a` completed?  Never
+// suspends the thread (try_wait may suspend it for a while when the phase is
+// incomplete; the copier must not be held up that way).
+__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase of parity `parity` of the mbarrier at `a`; gives up
 // (false) after kStageWaitNs, or early once another warp has given up
 // (*abort set) unless `drain`.
@@ -859,7 +875,7 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
         }
         const uint32_t seq = C.seq, slot = C.slot;
         const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
-        if (seq >= (uint32_t)kRing && !mbar_try(empty, (seq / kRing - 1u) & 1u)) return;
+        if (seq >= (uint32_t)kRing && !mbar_test(empty, (seq / kRing - 1u) & 1u)) return;
         const RJob &J = jobs[C.j];
         const int rows = C.rows, rx0 = C.rx0, ry0 = C.ry0;
         const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)rows;
@@ -890,12 +906,12 @@ template <typename T, int G>
 __device__ __forceinline__ bool wait_copying(uint32_t a, uint32_t parity, bool copier, const RJob *__restrict__ jobs,
                                              int njobs, int64_t total, const Plan *__restrict__ plans, const TSmem &S)
 {
-    if (mbar_try(a, parity)) return true;
-    if (!copier) return mbar_wait_slow(a, parity, S.abort, false);
+    if (!copier) return mbar_try(a, parity) || mbar_wait_slow(a, parity, S.abort, false);
+    if (mbar_test(a, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned n = 1;; ++n) {
         copy_ahead<T, G>(jobs, njobs, total, plans, S);
-        if (mbar_try(a, parity)) return true;
+        if (mbar_test(a, parity)) return true;
         if ((n & 15u) == 0 && (*reinterpret_cast<volatile int *>(S.abort) || globaltimer_ns() - t0 > kStageWaitNs))
             return false;
     }
