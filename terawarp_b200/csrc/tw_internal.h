@@ -87,6 +87,7 @@ constexpr int kKernErrTimeout = 1;
 // Source elements per TMA row copy of the staged TPS path (the tensor map's box
 // width; the staged box of a unit is at most this wide).
 constexpr int kStageBoxW = 96;
+constexpr int kStageBoxH = 28;
 
 // ---------------------------------------------------------------- TPS eval
 

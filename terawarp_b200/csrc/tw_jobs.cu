@@ -181,16 +181,16 @@ bool encode_source_map(RJob &j)
     const EncodeTiled fn = encode_fn();
     if (!fn || !j.src) return false;
     const uint64_t es = j.dtype == TW_U8 ? 1 : 2;
-    // TMA rules: 16-byte aligned base and row / plane pitches; a box no wider
-    // than the tensor
+    // TMA rules: 16-byte aligned base and row / plane pitches; a box (one
+    // staged plane: kStageBoxW x kStageBoxH elements) no larger than the tensor
     if (reinterpret_cast<uintptr_t>(j.src) % 16 != 0) return false;
     if ((j.src_py * es) % 16 != 0 || (j.src_pz * es) % 16 != 0) return false;
-    if (j.src_n[0] < kStageBoxW || j.src_n[1] < 1 || j.src_n[2] < 1) return false;
+    if (j.src_n[0] < kStageBoxW || j.src_n[1] < kStageBoxH || j.src_n[2] < 1) return false;
     if (j.src_n[0] > 0xffffffffLL || j.src_n[1] > 0xffffffffLL || j.src_n[2] > 0xffffffffLL) return false;
     if ((uint64_t)j.src_pz * es >= (1ull << 40)) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)j.src_n[0], (cuuint64_t)j.src_n[1], (cuuint64_t)j.src_n[2]};
     const cuuint64_t strides[2] = {(cuuint64_t)j.src_py * es, (cuuint64_t)j.src_pz * es};
-    const cuuint32_t box[3] = {(cuuint32_t)kStageBoxW, 1, 1};
+    const cuuint32_t box[3] = {(cuuint32_t)kStageBoxW, (cuuint32_t)kStageBoxH, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = fn(&j.tmap, es == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3,
                           const_cast<void *>(j.src), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,

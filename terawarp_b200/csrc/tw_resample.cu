@@ -568,7 +568,7 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // first and lists the walks that do not fit.  In the staged kernel warp 0
 // also copies the box's rows of every source plane its CTA's walks read, in
 // order, into a ring of kRing plane slots by TMA (cp.async.bulk.tensor, one
-// row per copy, from this GPU's own memory; no multicast).  Each slot has a
+// kBoxW x kHMax box per plane, from this GPU's own memory; no multicast).  Each slot has a
 // "full" mbarrier (transaction count of the copies) and an "empty" mbarrier
 // (one arrival per warp once no later plane of that warp reads the slot).
 // Warp 0 never blocks on its copier role: between its own planes, and while
@@ -576,10 +576,11 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // so copies run up to kRing - W planes ahead of the slowest warp and no warp
 // waits for another except through the data.
 // Slot 0 is copied a second time past the last slot,
-// so the z+1 tap of any plane is at a fixed offset.  The slots' row pitch is
-// 128 elements: a row or plane step moves an address by a multiple of 32
-// banks, so a warp's loads hit distinct banks whichever rows and planes its
-// lanes read.  A walk whose box or window does not fit, a nearest-neighbour
+// so the z+1 tap of any plane is at a fixed offset.  A slot holds the box
+// densely (row pitch kBoxW); a plane step moves an address by a multiple of 32
+// banks.  Units are numbered z-fastest, so the walks of one column (which
+// share their halo planes) and of neighbouring columns (which share halo
+// rows) run at the same time on neighbouring CTAs and meet in L2.  A walk whose box or window does not fit, a nearest-neighbour
 // job, or a source buffer TMA cannot describe gathers from global memory
 // instead (the gather kernel), with the same positions and the same
 // trilinear arithmetic (trilerp2).
@@ -589,9 +590,8 @@ constexpr int kTBY = 16;                     // unit height (y): one warp per ro
 constexpr int kRowWarps = kTBY;
 constexpr int kTpsThreads = 32 * kRowWarps;
 constexpr int kBoxW = kStageBoxW;            // TMA box: source elements per row copy
-constexpr int kRowP = 128;                   // shared-memory row pitch (elements)
-constexpr int kHMax = 28;                    // staged rows per plane
-constexpr int kRing = 24;                    // plane slots (plus the mirror of slot 0)
+constexpr int kHMax = kStageBoxH;            // TMA box: rows per staged plane
+constexpr int kRing = 32;                    // plane slots (plus the mirror of slot 0)
 constexpr int kMinAhead = 2;                 // slots a walk's window leaves for copies in flight
 // a wait on a copy or on another warp that has not ended after this long is
 // an error (the kernel reports kKernErrTimeout and returns)
@@ -617,7 +617,7 @@ struct alignas(16) CopyState {
     int n;            // planes to copy for the frontier walk (0: not staged)
     int i;            // next plane of the frontier walk to copy
     int j;            // job of the frontier walk
-    int rows, rx0, ry0;  // the frontier walk's box
+    int rx0, ry0;     // the frontier walk's box corner
     int last_job;     // job whose tensor map was last acquired
     uint32_t seq;     // planes copied so far
     uint32_t slot;    // seq % kRing
@@ -628,12 +628,13 @@ struct TGeom {
     static constexpr int NX = kTBX / G + 3;       // node columns of a unit (G <= 64)
     static constexpr int NRW = 4 * NX;            // y-contracted nodes of one row and layer
     static constexpr int ES = (int)sizeof(T);
-    static constexpr int ROW_B = kRowP * ES;
+    static constexpr int ROW_B = kBoxW * ES;
     static constexpr int PLANE_B = kHMax * ROW_B;
     static constexpr int RING_B = (kRing + 1) * PLANE_B;
     static constexpr int NBAR = 2 * kRing;        // full[kRing], empty[kRing]
     static constexpr size_t smem_bytes =
         128 + (size_t)RING_B + 8 * NBAR + sizeof(CopyState) + sizeof(float4) * (size_t)(G + kRowWarps * NRW);
+    static_assert(PLANE_B % 128 == 0, "TMA destinations are 128-byte aligned");
     static_assert((8 * NBAR) % 16 == 0 && sizeof(Plan) % 16 == 0 && sizeof(CopyState) % 16 == 0,
                   "the weight table is float4-aligned");
 };
@@ -706,10 +707,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, const vol
     return mbar_try(a, parity) || mbar_wait_slow(a, parity, abort, false);
 }
 
-// One row of a staged plane: kBoxW elements at tensor coordinates (x, y, z)
-// of the job's source buffer (elements outside it read as 0) into shared
-// memory at dst; completion is counted on the mbarrier at mbar.
-__device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t mbar)
+// One staged plane: the kBoxW x kHMax box at tensor coordinates (x, y, z) of
+// the job's source buffer (elements outside it read as 0) into shared memory
+// at dst; completion is counted on the mbarrier at mbar.
+__device__ __forceinline__ void tma_plane(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t mbar)
 {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
@@ -729,7 +730,8 @@ struct TSmem {
     int *abort;           // set by a warp that gave up waiting
 };
 
-// Job and unit of flattened unit index u.
+// Job and unit of flattened unit index u (z fastest: consecutive units are
+// the walks of one column).
 struct Walk {
     int j;
     int64_t Ox, Oy, z0, z1;
@@ -741,8 +743,8 @@ __device__ __forceinline__ Walk walk_of(const RJob *jobs, int njobs, int64_t u)
     w.j = find_job(jobs, njobs, u);
     const RJob &J = jobs[w.j];
     const int64_t lu = u - J.brick_begin;
-    const int64_t bx = lu % J.bricks[0], t = lu / J.bricks[0];
-    const int64_t by = t % J.bricks[1], bz = t / J.bricks[1];
+    const int64_t bz = lu % J.bricks[2], t = lu / J.bricks[2];
+    const int64_t bx = t % J.bricks[0], by = t / J.bricks[0];
     w.Ox = J.out_o[0] + bx * kTBX;
     w.Oy = J.out_o[1] + by * kTBY;
     w.z0 = J.out_o[2] + bz * J.zs;
@@ -847,7 +849,7 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
             const int j = find_job(jobs, njobs, u);
             const RJob &J = jobs[j];
             const int64_t lu = u - J.brick_begin;
-            const int64_t z0 = J.out_o[2] + (lu / (J.bricks[0] * J.bricks[1])) * J.zs;
+            const int64_t z0 = J.out_o[2] + (lu % J.bricks[2]) * J.zs;
             if (P.staged && j != C.last_job)  // the descriptor was written by a copy
                 asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
             __syncwarp();
@@ -855,7 +857,6 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
                 C.n = P.staged ? P.nplanes : 0;
                 C.i = 0;
                 C.j = j;
-                C.rows = P.rows;
                 C.rx0 = P.rx0;
                 C.ry0 = P.ry0;
                 C.pfirst = z0 + P.a - J.src_o[2];
@@ -877,19 +878,16 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
         const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
         if (seq >= (uint32_t)kRing && !mbar_test(empty, (seq / kRing - 1u) & 1u)) return;
         const RJob &J = jobs[C.j];
-        const int rows = C.rows, rx0 = C.rx0, ry0 = C.ry0;
-        const uint32_t bytes1 = (uint32_t)(kBoxW * Gm::ES) * (uint32_t)rows;
+        const int rx0 = C.rx0, ry0 = C.ry0;
         const int pz = (int)(C.pfirst + i);
-        __syncwarp();
-        if (lane == 0) mbar_expect_tx(full, slot == 0 ? 2u * bytes1 : bytes1);
-        __syncwarp();
-        if (lane < rows) {
+        if (lane == 0) {
             // every warp's reads of the slot's previous plane happen before its
             // release of it; order them before the asynchronous write
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B + (uint32_t)(lane * Gm::ROW_B);
-            tma_row(d, &J.tmap, rx0, ry0 + lane, pz, full);
-            if (slot == 0) tma_row(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, rx0, ry0 + lane, pz, full);
+            mbar_expect_tx(full, (uint32_t)(slot == 0 ? 2 : 1) * (uint32_t)Gm::PLANE_B);
+            const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B;
+            tma_plane(d, &J.tmap, rx0, ry0, pz, full);
+            if (slot == 0) tma_plane(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, rx0, ry0, pz, full);
         }
         __syncwarp();
         if (lane == 0) {
@@ -1038,7 +1036,7 @@ __device__ __forceinline__ void plane_positions(const RowLayer &L, float4 wz, fl
 template <typename T>
 __device__ __forceinline__ uint32_t staged_off(uint32_t kxy, uint32_t omax, uint32_t cz, float mx, float my, float mz)
 {
-    constexpr uint32_t ROW_B = kRowP * sizeof(T), PLANE_B = kHMax * ROW_B;
+    constexpr uint32_t ROW_B = kBoxW * sizeof(T), PLANE_B = kHMax * ROW_B;
     const uint32_t t = __float_as_uint(mz) + cz;  // slot, or slot + kRing past the wrap
     const uint32_t slot = min(t, t - (uint32_t)kRing);
     const uint32_t o = slot * PLANE_B + __float_as_uint(my) * ROW_B + __float_as_uint(mx) * (uint32_t)sizeof(T) + kxy;
@@ -1062,7 +1060,7 @@ __device__ __forceinline__ uint32_t pair_staged(const unsigned char *sm, uint32_
                                                 float2 p0, float2 p1, float2 pz2, const Frame &f, const float (&wl)[3],
                                                 const float (&wh)[3], int nvalid)
 {
-    constexpr uint32_t ES = sizeof(T), ROW_B = kRowP * ES, PLANE_B = kHMax * ROW_B;
+    constexpr uint32_t ES = sizeof(T), ROW_B = kBoxW * ES, PLANE_B = kHMax * ROW_B;
     const float2 MM = f2(kMagic, kMagic);
     float2 m0, m1, mz, f0, f1, fz;
     bool ok0 = true, ok1 = true;

@@ -66,9 +66,11 @@ struct Batch {
 
 // Source-box bound for a tile from the hull of its sample positions.  With
 // align > 1 the box's x extent is widened (inside the volume) to a multiple of
-// `align` elements and to at least min_x, so that its rows meet the TMA rules
-// of the staged resample (16-byte pitches, rows no narrower than one copy).
-Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3], int64_t align = 1, int64_t min_x = 0)
+// `align` elements and to at least min_x, and its y extent to at least min_y,
+// so that it meets the TMA rules of the staged resample (16-byte pitches, no
+// narrower or lower than one staged plane).
+Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3], int64_t align = 1, int64_t min_x = 0,
+                  int64_t min_y = 0)
 {
     Box b;
     for (int a = 0; a < 3; ++a) {
@@ -90,6 +92,9 @@ Box box_from_hull(const float lo[3], const float hi[3], const int64_t sz[3], int
         const int64_t o = std::max<int64_t>(0, std::min(b.o[0], sz[0] - w));
         b.o[0] = o;
         b.n[0] = w;
+        const int64_t hgt = std::min(sz[1], std::max(b.n[1], min_y));
+        b.o[1] = std::max<int64_t>(0, std::min(b.o[1], sz[1] - hgt));
+        b.n[1] = hgt;
     }
     return b;
 }
@@ -176,7 +181,7 @@ tw_status run_tiled(tw_ctx *ctx, int kind, const float4 *nodes, int g, const dou
         std::vector<float> lo, hi;
         TW_TRY(tps_box_hull(ctx, nodes, gsz, g, cb, ctx->stream, lo, hi));
         for (int64_t t = 0; t < ntiles; ++t)
-            srcs[t] = box_from_hull(&lo[3 * t], &hi[3 * t], src_sz, 16 / (int64_t)es, kStageBoxW);
+            srcs[t] = box_from_hull(&lo[3 * t], &hi[3 * t], src_sz, 16 / (int64_t)es, kStageBoxW, kStageBoxH);
     } else {
         for (int64_t t = 0; t < ntiles; ++t) {
             float lo[3], hi[3];
