@@ -882,8 +882,8 @@ __device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t tot
         const int pz = (int)(C.pfirst + i);
         if (lane == 0) {
             // every warp's reads of the slot's previous plane happen before its
-            // release of it; order them before the asynchronous write
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            // arrival on the slot's empty barrier (a release), which this warp
+            // observed (an acquire) before issuing the asynchronous write
             mbar_expect_tx(full, (uint32_t)(slot == 0 ? 2 : 1) * (uint32_t)Gm::PLANE_B);
             const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B;
             tma_plane(d, &J.tmap, rx0, ry0, pz, full);
