@@ -240,16 +240,17 @@ __global__ void k_fill_a(const double *__restrict__ ctr, int n, const double *__
 // UPDATE(i, j, k) subtracts L(i,k) L(j,k)' from tile (i, j) once both panel
 // tiles exist and the tile's previous update is in.  The back substitution
 // is DIAG(kb) (the diagonal block's triangular solve) and BACK(ib, kb) (the
-// rows of block ib) in the same way.  Tasks are numbered in one order that
-// respects every dependency (step by step; within a step POTRF, the panel,
-// then the updates column by column, so the next panel's tiles come first),
-// and CTA c takes tasks c, c + G, c + 2G, ... in that order; as all CTAs are
-// resident (cooperative launch), the lowest unfinished task can always run,
-// so the schedule cannot deadlock.  A step's critical path is then one
-// POTRF, one TRSM and one UPDATE instead of two grid-wide barriers, and
-// later steps start while earlier ones finish.  L1 is not coherent across
-// SMs within a kernel, so every load of data another CTA wrote (A, z)
-// bypasses L1 (__ldcg).
+// rows of block ib) in the same way.
+//
+// The critical path is the chain POTRF(k-1) -> TRSM(k, k-1) -> UPDATE(k, k,
+// k-1) -> POTRF(k): CTA 0 runs only that chain, one fused step per k with
+// its three tiles kept in shared memory, and then the back substitution's
+// chain.  The other CTAs take every other task in one order that respects
+// every dependency, CTA c taking every (G-1)-th; as all CTAs are resident
+// (cooperative launch) and every wait of a task is on tasks earlier in that
+// order, the lowest unfinished task can always run, so the schedule cannot
+// deadlock.  L1 is not coherent across SMs within a kernel, so every load of
+// data another CTA wrote (A, z) bypasses L1 (__ldcg).
 
 constexpr int kSolveThreads = 256;
 constexpr int kStTimeout = 4;
@@ -326,110 +327,129 @@ __device__ __forceinline__ void signal_done(int *flag, int value)
     }
 }
 
-// potrf of diagonal block kb: thread t holds its 4 x 4 patch (rows tr + 16u,
-// columns tc + 16v) of the block in registers.  In step j the pivot's owner
-// publishes it; the owners of column j scale their elements of it (x
-// rsqrt(pivot)) and publish them; every thread then updates its patch of the
-// trailing lower triangle from the published column.  Two CTA barriers per
-// column and no shared-memory read-modify-write.
-__device__ void potrf_tile(double *__restrict__ A, int m, int kb, int *status, double *sm)
+// Column J onwards of the Cholesky of a 16 x 16 block held by the lanes of
+// one warp, lane l (l = lane % 16) owning row l (v[k] = element (l, k)): the
+// pivot comes from its row's lane, the scaled column goes to the other lanes
+// by shuffles.  Compile-time recursion over the columns keeps every index of
+// v constant, so v stays in registers.
+template <int J>
+__device__ __forceinline__ void panel_factor(double (&v)[16], int l, int lane, int *status)
 {
-    double *col = sm;        // column j, scaled
-    double *piv = sm + kNB;  // pivot of column j
-    const int r0 = kb * kNB;
-    const int nb = min(kNB, m - r0);
-    const int t = threadIdx.x;
-    const int tr = t >> 4, tc = t & 15;
-    double a[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int r = tr + 16 * u, c = tc + 16 * v;
-            a[u][v] = (r < nb && c < nb) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
-        }
-    __syncthreads();  // sm is free (the caller's previous task may still read it)
-#pragma unroll 1
-    for (int j = 0; j < kNB; ++j) {
-        const int uj = j >> 4, cj = j & 15;
-        // the pivot's owner: row j, column j
-        if (tr == cj && tc == cj) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (u == uj) piv[0] = a[u][u];
-        }
-        __syncthreads();
-        double d = piv[0];
+    if constexpr (J < 16) {
+        const unsigned full = 0xffffffffu;
+        double d = __shfl_sync(full, v[J], J);  // the pivot, from its row's lane
         if (!(d > 0.0)) {
-            if (t == 0) atomicOr(status, kStNotSPD);
+            if (lane == 0) atomicOr(status, kStNotSPD);
             d = 1.0;
         }
         const double inv = rsqrt(d);
-        if (tc == cj) {
-            // this thread owns column j at rows tr + 16u
+        if (l > J) v[J] *= inv;
+        else if (l == J) v[J] = d * inv;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v)
-                    if (v == uj) {
-                        const int i = tr + 16 * u;
-                        if (i > j) {
-                            a[u][v] *= inv;
-                            col[i] = a[u][v];
-                        } else if (i == j) {
-                            a[u][v] = d * inv;
-                        }
-                    }
+        for (int k = J + 1; k < 16; ++k) {
+            const double lkj = __shfl_sync(full, v[J], k);  // L(k, J), from row k's lane
+            if (l >= k) v[k] -= v[J] * lkj;
         }
-        __syncthreads();
-        double ci[4], cl[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            ci[u] = col[tr + 16 * u];
-            cl[u] = col[tc + 16 * u];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const int i = tr + 16 * u, l = tc + 16 * v;
-                if (l > j && i >= l) a[u][v] -= ci[u] * cl[v];
-            }
+        panel_factor<J + 1>(v, l, lane, status);
     }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int r = tr + 16 * u, c = tc + 16 * v;
-            if (r < nb && c < nb) A[(size_t)(r0 + r) * m + r0 + c] = c <= r ? a[u][v] : 0.0;
-        }
 }
 
-// trsm of row block ib against diagonal block kb: L(ib,kb) = A(ib,kb) L(kb,kb)^-T.
-// Rows are independent: the four lanes (q = lane & 3) of one row keep its
-// columns q, q+4, .. in registers; column c is finished by its owner (x
-// 1/L(c,c)), handed to the other three by a warp shuffle, and subtracted from
-// the later columns: X(r,c') -= X(r,c) L(c',c).  No CTA barrier inside the
-// column loop.
-__device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double *sm)
+// Cholesky of a diagonal tile held in shared memory (lower triangle of
+// a[kNB][kNB + 1]; padding rows and columns hold the identity), in four
+// 16-column panels: warp 0 factors the panel's 16 x 16 diagonal block in
+// registers (lane l < 16 owns its row l; each finished column goes to the
+// other lanes by shuffles), then every thread solves the panel's rows below
+// it (four lanes per row) and applies the trailing update.  rdiag gets the
+// reciprocals of the diagonal.  Three CTA barriers per panel.
+__device__ void potrf_smem(double (*a)[kNB + 1], double *rdiag, int *status)
 {
-    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
-    double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
-    double *rdiag = sm + 2 * kNB * (kNB + 1) + 2 * kNB;
-    const int nblk = (m + kNB - 1) / kNB;
-    const int r0 = kb * kNB;
-    const int i0 = row_block_start(ib, nblk, m);
-    const int nbk = min(kNB, m - r0);
-    const int nbi = row_block_rows(ib, nblk, m);
-    __syncthreads();
+    const int t = threadIdx.x, lane = t & 31;
+    const unsigned full = 0xffffffffu;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kNB; c0 += 16) {
+        if (t < 32) {
+            const int l = lane & 15;
+            double v[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) v[k] = k <= l ? a[c0 + l][c0 + k] : 0.0;
+            panel_factor<0>(v, l, lane, status);
+            if (lane < 16) {
+                double dl = 1.0;  // v[l], selected without a run-time index (v stays in registers)
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    if (k <= l) a[c0 + l][c0 + k] = v[k];
+                    if (k == l) dl = v[k];
+                }
+                rdiag[c0 + l] = 1.0 / dl;
+            }
+        }
+        __syncthreads();
+        const int nr = kNB - c0 - 16;  // rows below the panel's diagonal block
+        {
+            // X(i, c0 + c) = (A(i, c0 + c) - sum_{k<c} X(i, c0 + k) L(c0 + c, c0 + k)) / L(c0 + c, c0 + c)
+            const int r = t >> 2, q = t & 3, base = lane & ~3;
+            const bool act = r < nr;
+            const int i = c0 + 16 + (act ? r : 0);
+            double x[4];
+#pragma unroll
+            for (int k4 = 0; k4 < 4; ++k4) x[k4] = act ? a[i][c0 + 4 * k4 + q] : 0.0;
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const double mine = x[c >> 2] * rdiag[c0 + c];  // meaningful in the owner lane only
+                const double xc = __shfl_sync(full, mine, base | (c & 3));
+                if (act && q == (c & 3)) a[i][c0 + c] = xc;
+#pragma unroll
+                for (int k4 = 0; k4 < 4; ++k4) {
+                    const int cp = 4 * k4 + q;
+                    if (cp > c) x[k4] -= xc * a[c0 + cp][c0 + c];
+                }
+            }
+        }
+        __syncthreads();
+        for (int e = t; e < nr * nr; e += blockDim.x) {
+            const int ii = e / nr, jj = e % nr;
+            if (jj <= ii) {
+                const int i = c0 + 16 + ii, j = c0 + 16 + jj;
+                double acc = 0.0;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) acc += a[i][c0 + k] * a[j][c0 + k];
+                a[i][j] -= acc;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Loads tile (row block ib, column block jb) of A into t (rows x cols of it
+// valid; the rest: identity on the diagonal when `diag`, else zero).
+__device__ void load_tile(double (*t)[kNB + 1], const double *__restrict__ A, int m, int i0, int rows, int j0, int cols,
+                          bool diag)
+{
 #pragma unroll 4
     for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-        int r = e / kNB, c = e % kNB;
-        L[r][c] = (r < nbk && c < nbk) ? __ldcg(&A[(size_t)(r0 + r) * m + r0 + c]) : (r == c ? 1.0 : 0.0);
-        X[r][c] = (r < nbi && c < nbk) ? __ldcg(&A[(size_t)(i0 + r) * m + r0 + c]) : 0.0;
+        const int r = e / kNB, c = e % kNB;
+        t[r][c] = (r < rows && c < cols) ? __ldcg(&A[(size_t)(i0 + r) * m + j0 + c])
+                                         : ((diag && r == c) ? 1.0 : 0.0);
     }
-    __syncthreads();
-    if (threadIdx.x < kNB) rdiag[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
+}
+
+__device__ void store_tile(double *__restrict__ A, int m, const double (*t)[kNB + 1], int i0, int rows, int j0, int cols,
+                           bool lower)
+{
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        const int r = e / kNB, c = e % kNB;
+        if (r < rows && c < cols) A[(size_t)(i0 + r) * m + j0 + c] = (!lower || c <= r) ? t[r][c] : 0.0;
+    }
+}
+
+// X = X L^-T for a tile X in shared memory against a factored diagonal tile
+// L (rdiag: reciprocals of its diagonal), nbk valid columns.  Rows are
+// independent: the four lanes (q = lane & 3) of one row keep its columns q,
+// q+4, .. in registers; column c is finished by its owner (x 1/L(c,c)),
+// handed to the other three by a warp shuffle, and subtracted from the later
+// columns: X(r,c') -= X(r,c) L(c',c).  No CTA barrier inside the column loop.
+__device__ void trsm_smem(const double (*L)[kNB + 1], double (*X)[kNB + 1], const double *rdiag, int nbk)
+{
     const int lane = threadIdx.x & 31;
     const int r = (threadIdx.x >> 5) * 8 + (lane >> 2);  // 8 rows per warp
     const int q = lane & 3;
@@ -437,13 +457,12 @@ __device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double 
     double x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = X[r][4 * k + q];
-    __syncthreads();  // rdiag is visible
     // fully unrolled so that every index into x is a constant (x stays in
     // registers); columns at or beyond nbk are skipped
 #pragma unroll
     for (int c = 0; c < kNB; ++c) {
         if (c >= nbk) break;
-        const double mine = x[c >> 2] * rdiag[c];           // meaningful in the owner lane only
+        const double mine = x[c >> 2] * rdiag[c];  // meaningful in the owner lane only
         const double xc = __shfl_sync(0xffffffffu, mine, base | (c & 3));
         if (q == (c & 3)) X[r][c] = xc;
 #pragma unroll
@@ -452,11 +471,52 @@ __device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double 
             if (cp > c && cp < nbk) x[k] -= xc * L[cp][c];
         }
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-        int rr = e / kNB, c = e % kNB;
-        if (rr < nbi && c < nbk) A[(size_t)(i0 + rr) * m + r0 + c] = X[rr][c];
+}
+
+// acc[u][v] = sum_p Li(tr + 16u, p) Lj(tc + 16v, p) over nbk columns, thread
+// (tr, tc) = (t / 16, t % 16): conflict-free reads of Lj with the 65-double pitch.
+__device__ __forceinline__ void syrk_acc(const double (*Li)[kNB + 1], const double (*Lj)[kNB + 1], int nbk,
+                                         double (&acc)[4][4])
+{
+    const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+    for (int p = 0; p < nbk; ++p) {
+        double a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = Li[tr + 16 * u][p];
+            b[u] = Lj[tc + 16 * u][p];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
     }
+}
+
+// trsm of row block ib against diagonal block kb: L(ib,kb) = A(ib,kb) L(kb,kb)^-T.
+__device__ void trsm_tile(double *__restrict__ A, int m, int kb, int ib, double *sm)
+{
+    double(*L)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
+    double *rdiag = sm + 2 * kNB * (kNB + 1);
+    const int nblk = (m + kNB - 1) / kNB;
+    const int r0 = kb * kNB;
+    const int i0 = row_block_start(ib, nblk, m);
+    const int nbk = min(kNB, m - r0);
+    const int nbi = row_block_rows(ib, nblk, m);
+    __syncthreads();
+    load_tile(L, A, m, r0, nbk, r0, nbk, true);
+    load_tile(X, A, m, i0, nbi, r0, nbk, false);
+    __syncthreads();
+    if (threadIdx.x < kNB) rdiag[threadIdx.x] = 1.0 / L[threadIdx.x][threadIdx.x];
+    __syncthreads();
+    trsm_smem(L, X, rdiag, nbk);
+    __syncthreads();
+    store_tile(A, m, X, i0, nbi, r0, nbk, false);
 }
 
 // Trailing update of tile (ib, jb) at step kb: A(ib,jb) -= L(ib,kb) L(jb,kb)' for
@@ -470,28 +530,12 @@ __device__ void syrk_tile(double *__restrict__ A, int m, int kb, int ib, int jb,
     const int r0 = kb * kNB, i0 = row_block_start(ib, nblk, m), j0 = jb * kNB;
     const int nbk = min(kNB, m - r0), nbi = row_block_rows(ib, nblk, m), nbj = min(kNB, m - j0);
     __syncthreads();
-#pragma unroll 4
-    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
-        int r = e / kNB, c = e % kNB;
-        Li[r][c] = (r < nbi && c < nbk) ? __ldcg(&A[(size_t)(i0 + r) * m + r0 + c]) : 0.0;
-        Lj[r][c] = (r < nbj && c < nbk) ? __ldcg(&A[(size_t)(j0 + r) * m + r0 + c]) : 0.0;
-    }
+    load_tile(Li, A, m, i0, nbi, r0, nbk, false);
+    load_tile(Lj, A, m, j0, nbj, r0, nbk, false);
     __syncthreads();
-    // rows tr + 16u, columns tc + 16v (conflict-free reads of Lj, see potrf_tile)
+    double acc[4][4];
+    syrk_acc(Li, Lj, nbk, acc);
     const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
-    double acc[4][4] = {};
-    for (int p = 0; p < nbk; ++p) {
-        double a[4], b[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            a[u] = Li[tr + 16 * u][p];
-            b[u] = Lj[tc + 16 * u][p];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
-    }
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -560,30 +604,96 @@ __device__ void bwd_update(const double *__restrict__ A, int m, int kb, int ib, 
     }
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict__ A, int m, double *__restrict__ Z,
-                                                              int *status, int *flags, unsigned long long limit_ns)
+// CTA 0: the critical chain.  Step k fuses TRSM(k, k-1), UPDATE(k, k, k-1)
+// and POTRF(k), keeping the factored diagonal tile, the new panel tile and
+// the next diagonal tile in shared memory; then the back substitution's
+// chain DIAG(kb), BACK(kb - 1, kb).
+__device__ void solve_chain(double *__restrict__ A, int m, double *__restrict__ z, int *status, SolveFlags *F,
+                            int *tdone, int *cnt, int *bcnt, unsigned long long limit_ns, double *sm)
 {
-    extern __shared__ double sm[];
     const int nblk = (m + kNB - 1) / kNB;
-    SolveFlags *F = reinterpret_cast<SolveFlags *>(flags);
-    int *tdone = flags + 4;
-    int *cnt = tdone + nblk + 1;
-    int *bcnt = cnt + (nblk + 1) * nblk;
-    double *z = Z + 16;  // z(4:), 4 per row; y' then x' overwrite it
-    const long long G = gridDim.x, bid = blockIdx.x;
+    double(*Ld)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm);
+    double(*X)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + kNB * (kNB + 1));
+    double(*Ad)[kNB + 1] = reinterpret_cast<double(*)[kNB + 1]>(sm + 2 * kNB * (kNB + 1));
+    double *rdiag = sm + 3 * kNB * (kNB + 1);
+    {
+        const int nb = min(kNB, m);
+        load_tile(Ld, A, m, 0, nb, 0, nb, true);
+        __syncthreads();
+        potrf_smem(Ld, rdiag, status);
+        store_tile(A, m, Ld, 0, nb, 0, nb, true);
+        signal_done(&F->pdone, 1);
+    }
+    for (int k = 1; k < nblk; ++k) {
+        const int r0 = (k - 1) * kNB, i0 = k * kNB, nbi = min(kNB, m - i0);
+        // TRSM(k, k-1): X = A(k, k-1) L(k-1, k-1)^-T
+        if (!wait_ge(&cnt[k * nblk + k - 1], k - 1, F, status, limit_ns)) return;
+        load_tile(X, A, m, i0, nbi, r0, kNB, false);
+        __syncthreads();
+        trsm_smem(Ld, X, rdiag, kNB);
+        __syncthreads();
+        store_tile(A, m, X, i0, nbi, r0, kNB, false);
+        signal_done(&tdone[k], k);
+        // UPDATE(k, k, k-1): A(k, k) -= X X'
+        if (!wait_ge(&cnt[k * nblk + k], k - 1, F, status, limit_ns)) return;
+        load_tile(Ad, A, m, i0, nbi, i0, nbi, true);
+        __syncthreads();
+        {
+            double acc[4][4];
+            syrk_acc(X, X, kNB, acc);
+            const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int r = tr + 16 * u, c = tc + 16 * v;
+                    if (r < nbi && c <= r) Ad[r][c] -= acc[u][v];
+                }
+        }
+        __syncthreads();
+        // POTRF(k)
+        potrf_smem(Ad, rdiag, status);
+        store_tile(A, m, Ad, i0, nbi, i0, nbi, true);
+        signal_done(&F->pdone, k + 1);
+        double(*t)[kNB + 1] = Ld;
+        Ld = Ad;
+        Ad = t;
+    }
+    for (int kb = nblk - 1; kb >= 0; --kb) {
+        if (!wait_ge(&tdone[nblk], kb + 1, F, status, limit_ns) ||
+            !wait_ge(&bcnt[kb], nblk - 1 - kb, F, status, limit_ns))
+            return;
+        bwd_diag(A, m, kb, z, sm);
+        signal_done(&F->ddone, nblk - kb);
+        if (kb >= 1) {
+            if (!wait_ge(&bcnt[kb - 1], nblk - 1 - kb, F, status, limit_ns)) return;
+            bwd_update(A, m, kb, kb - 1, z, sm);
+            signal_done(&bcnt[kb - 1], nblk - kb);
+        }
+    }
+}
+
+// CTAs 1 .. G-1: every other task, in one order that respects every
+// dependency, CTA c taking every (G-1)-th.  Step k: the panel tiles TRSM(i, k)
+// of rows i >= k + 2 (and the right-hand-side block), then the updates
+// UPDATE(i, j, k) column by column, without the chain's UPDATE(k+1, k+1, k).
+// Then the back substitution's BACK(ib, kb) for ib <= kb - 2.
+__device__ void solve_others(double *__restrict__ A, int m, double *__restrict__ z, int *status, SolveFlags *F,
+                             int *tdone, int *cnt, int *bcnt, unsigned long long limit_ns, double *sm)
+{
+    const int nblk = (m + kNB - 1) / kNB;
+    const long long G = gridDim.x - 1, bid = blockIdx.x - 1;
     long long base = 0;  // number of the step's first task
     for (int k = 0; k < nblk; ++k) {
-        const int nt = nblk - k;  // panel tiles: row blocks k+1 .. nblk
-        long long nu = 0;         // updates: column blocks j = k+1 .. nblk-1, row blocks j .. nblk
-        for (int j = k + 1; j < nblk; ++j) nu += nblk + 1 - j;
-        const long long count = 1 + nt + nu;
+        const int lo_i = k + 1 < nblk ? k + 2 : k + 1;
+        const int nt = nblk - lo_i + 1;
+        const int first = k + 1 < nblk ? nblk - k - 1 : 0;  // updates of column block k+1, rows k+2 .. nblk
+        long long nu = first;
+        for (int j = k + 2; j < nblk; ++j) nu += nblk + 1 - j;
+        const long long count = nt + nu;
         for (long long e = ((bid - base) % G + G) % G; e < count; e += G) {
-            if (e == 0) {
-                if (!wait_ge(&cnt[k * nblk + k], k, F, status, limit_ns)) return;
-                potrf_tile(A, m, k, status, sm);
-                signal_done(&F->pdone, k + 1);
-            } else if (e <= nt) {
-                const int i = k + (int)e;
+            if (e < nt) {
+                const int i = lo_i + (int)e;
                 if (!wait_ge(&F->pdone, k + 1, F, status, limit_ns) ||
                     !wait_ge(&cnt[i * nblk + k], k, F, status, limit_ns))
                     return;
@@ -597,13 +707,20 @@ __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict
                 }
                 signal_done(&tdone[i], k + 1);
             } else {
-                long long f = e - 1 - nt;
-                int j = k + 1;
-                while (f >= nblk + 1 - j) {
-                    f -= nblk + 1 - j;
-                    ++j;
+                long long f = e - nt;
+                int i, j;
+                if (f < first) {
+                    j = k + 1;
+                    i = k + 2 + (int)f;
+                } else {
+                    f -= first;
+                    j = k + 2;
+                    while (f >= nblk + 1 - j) {
+                        f -= nblk + 1 - j;
+                        ++j;
+                    }
+                    i = j + (int)f;
                 }
-                const int i = j + (int)f;
                 if (!wait_ge(&tdone[i], k + 1, F, status, limit_ns) ||
                     !wait_ge(&tdone[j], k + 1, F, status, limit_ns) ||
                     !wait_ge(&cnt[i * nblk + j], k, F, status, limit_ns))
@@ -614,32 +731,35 @@ __global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict
         }
         base += count;
     }
-    // back substitution L' x = y, block by block from the last: DIAG(kb)
-    // needs y'(kb) (TRSM(nblk, kb)) and every BACK(kb, kb') for kb' > kb;
-    // BACK(ib, kb) needs DIAG(kb) and the block's previous BACK
     for (int kb = nblk - 1; kb >= 0; --kb) {
-        const long long count = 1 + kb;  // DIAG(kb), then BACK(ib, kb) for ib = kb-1 .. 0
+        const long long count = kb >= 2 ? kb - 1 : 0;  // BACK(ib, kb) for ib = kb-2 .. 0
         for (long long e = ((bid - base) % G + G) % G; e < count; e += G) {
-            if (e == 0) {
-                if (!wait_ge(&tdone[nblk], kb + 1, F, status, limit_ns) ||
-                    !wait_ge(&bcnt[kb], nblk - 1 - kb, F, status, limit_ns))
-                    return;
-                bwd_diag(A, m, kb, z, sm);
-                signal_done(&F->ddone, nblk - kb);
-            } else {
-                const int ib = kb - (int)e;
-                if (!wait_ge(&F->ddone, nblk - kb, F, status, limit_ns) ||
-                    !wait_ge(&bcnt[ib], nblk - 1 - kb, F, status, limit_ns))
-                    return;
-                bwd_update(A, m, kb, ib, z, sm);
-                signal_done(&bcnt[ib], nblk - kb);
-            }
+            const int ib = kb - 2 - (int)e;
+            if (!wait_ge(&F->ddone, nblk - kb, F, status, limit_ns) ||
+                !wait_ge(&bcnt[ib], nblk - 1 - kb, F, status, limit_ns))
+                return;
+            bwd_update(A, m, kb, ib, z, sm);
+            signal_done(&bcnt[ib], nblk - kb);
         }
         base += count;
     }
 }
 
-constexpr size_t kSolveSmem = sizeof(double) * (2 * kNB * (kNB + 1) + 3 * kNB);
+__global__ void __launch_bounds__(kSolveThreads) k_chol_solve(double *__restrict__ A, int m, double *__restrict__ Z,
+                                                              int *status, int *flags, unsigned long long limit_ns)
+{
+    extern __shared__ double sm[];
+    const int nblk = (m + kNB - 1) / kNB;
+    SolveFlags *F = reinterpret_cast<SolveFlags *>(flags);
+    int *tdone = flags + 4;
+    int *cnt = tdone + nblk + 1;
+    int *bcnt = cnt + (nblk + 1) * nblk;
+    double *z = Z + 16;  // z(4:), 4 per row; y' then x' overwrite it
+    if (blockIdx.x == 0) solve_chain(A, m, z, status, F, tdone, cnt, bcnt, limit_ns, sm);
+    else solve_others(A, m, z, status, F, tdone, cnt, bcnt, limit_ns, sm);
+}
+
+constexpr size_t kSolveSmem = sizeof(double) * (3 * kNB * (kNB + 1) + 3 * kNB);
 
 // 4c. c = H1 H2 H3 H4 [0; w]  (Z rows 0..3 are replaced by zeros)
 __global__ void k_apply_q(int n, const double *V, const double *tau, const double *Z, double *C)
