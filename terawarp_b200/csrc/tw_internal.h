@@ -84,10 +84,13 @@ void brick_dims(int kind, int g, int64_t out[3]);
 bool encode_source_map(RJob &j);
 // Device error word bits set by the resample kernels.
 constexpr int kKernErrTimeout = 1;
-// Source elements per TMA row copy of the staged TPS path (the tensor map's box
-// width; the staged box of a unit is at most this wide).
-constexpr int kStageBoxW = 96;
-constexpr int kStageBoxH = 28;
+// The TMA box of the staged TPS path: source elements per staged row and rows
+// per staged plane (the staged box of a unit is at most this large).  A row
+// of 128 elements keeps the row pitch in shared memory a multiple of 32
+// banks, so a warp whose taps straddle two rows reads them without bank
+// conflicts.
+constexpr int kStageBoxW = 128;
+constexpr int kStageBoxH = 32;
 
 // ---------------------------------------------------------------- TPS eval
 

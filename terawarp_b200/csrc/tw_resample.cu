@@ -39,7 +39,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kTX = 32;
-constexpr int kTY = 8;
 constexpr int kV = 8;                 // voxels per lane per brick row (4 pairs)
 constexpr int kBX = kTX * kV;         // 256 voxels per brick along x
 constexpr float kMagic = 12582912.0f; // 1.5 * 2^23: add.rm(q, kMagic) = kMagic + floor(q)
@@ -304,27 +303,6 @@ __device__ __forceinline__ float mag(const T *p)
     return __int_as_float(0x4B000000 | (int)(uint32_t)__ldg(p));
 }
 
-// Per-lane constants of the packed path: weight pairs for the two voxels.
-struct PairW {
-    float2 w0[4];  // (w_a(0), w_a(0))
-    float2 w1[4];  // (w_a(1), w_a(1))
-    float2 wz[4];  // (w_a(0), w_a(1))
-};
-
-__device__ __forceinline__ PairW make_pairw(const float4 (&wx)[2])
-{
-    PairW p;
-    const float a0[4] = {wx[0].x, wx[0].y, wx[0].z, wx[0].w};
-    const float a1[4] = {wx[1].x, wx[1].y, wx[1].z, wx[1].w};
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        p.w0[a] = f2(a0[a], a0[a]);
-        p.w1[a] = f2(a1[a], a1[a]);
-        p.wz[a] = f2(a0[a], a1[a]);
-    }
-    return p;
-}
-
 // The four source rows a trilinear sample reads, (dy, dz) = (r & 1, r >> 1),
 // as base pointers of one brick, plus the int32 pitches.  The bases sit at
 // the low corner of the brick's sample hull, so every unchecked tap is a
@@ -565,39 +543,55 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // plus the +1 tap -- is a box of at most kBoxW x kHMax elements per source
 // plane and a window of W planes that slides down one plane per output
 // plane.  A planning kernel (one warp per walk) computes every walk's plan
-// first and lists the walks that do not fit.  In the staged kernel warp 0
-// also copies the box's rows of every source plane its CTA's walks read, in
-// order, into a ring of kRing plane slots by TMA (cp.async.bulk.tensor, one
-// kBoxW x kHMax box per plane, from this GPU's own memory; no multicast).  Each slot has a
-// "full" mbarrier (transaction count of the copies) and an "empty" mbarrier
-// (one arrival per warp once no later plane of that warp reads the slot).
-// Warp 0 never blocks on its copier role: between its own planes, and while
-// it waits, it issues every copy whose slot has been released by all warps,
-// so copies run up to kRing - W planes ahead of the slowest warp and no warp
-// waits for another except through the data.
-// Slot 0 is copied a second time past the last slot,
-// so the z+1 tap of any plane is at a fixed offset.  A slot holds the box
-// densely (row pitch kBoxW); a plane step moves an address by a multiple of 32
-// banks.  Units are numbered z-fastest, so the walks of one column (which
-// share their halo planes) and of neighbouring columns (which share halo
-// rows) run at the same time on neighbouring CTAs and meet in L2.  A walk whose box or window does not fit, a nearest-neighbour
-// job, or a source buffer TMA cannot describe gathers from global memory
-// instead (the gather kernel), with the same positions and the same
-// trilinear arithmetic (trilerp2).
+// first and lists the walks that do not fit.  The staged kernel's CTA has
+// one producer warp next to the 16 row warps: it copies the box of every
+// source plane its CTA's walks read, in order, into a ring of kRing plane
+// slots by TMA (cp.async.bulk.tensor, one kBoxW x kHMax box per plane, from
+// this GPU's own memory; no multicast).  Each slot has a "full" mbarrier
+// (transaction count of the copies) and an "empty" mbarrier (one arrival per
+// row warp once no later plane of that warp reads the slot); the producer
+// waits on "empty" before it reuses a slot, so copies run up to kRing - W
+// planes ahead of the slowest row warp and no row warp waits for another
+// except through the data.  Slot 0 is copied a second time past the last
+// slot, so the z+1 tap of any plane is at a fixed offset.  A slot holds the
+// box densely (row pitch kBoxW).  Units are numbered z-fastest, so the walks
+// of one column (which share their halo planes) and of neighbouring columns
+// (which share halo rows) run at the same time on neighbouring CTAs and meet
+// in L2.  A walk whose box or window does not fit, a nearest-neighbour job,
+// or a source buffer TMA cannot describe gathers from global memory instead
+// (the gather kernel), with the same positions and the same trilinear
+// arithmetic (trilerp2).
+//
+// Interior walks.  The planning kernel also marks a walk "interior" when
+// every tap of every voxel lies inside the subject volume and the source
+// buffer and the unit lies wholly inside the output region.  Row warps then
+// skip every range test: per cell layer only the node contractions, per
+// output plane only positions, staged taps, lerps and one store.  Other
+// walks apply the reference's range rule voxel by voxel.
 
 constexpr int kTBX = 64;                     // unit width (x): 32 lanes x 2 voxels
 constexpr int kTBY = 16;                     // unit height (y): one warp per row
-constexpr int kRowWarps = kTBY;
-constexpr int kTpsThreads = 32 * kRowWarps;
+constexpr int kTpsThreads = 32 * kTBY;        // gather kernel: one warp per output row
+// staged kernel: output rows per row warp.  One row per warp, 16 row warps
+// and the producer (17 warps, 96 registers a thread) measured 17.9 ms on the
+// 2048 x 2048 x 1024 u16 job against 20.5 ms for two rows per warp (9 warps,
+// 168 registers): more warps hide the dependency chains better than the
+// second row's independent work does.
+constexpr int kRowsPerWarp = 1;
+constexpr int kRowWarps = kTBY / kRowsPerWarp;  // row warp y owns rows y + k kRowWarps
+constexpr int kStagedThreads = 32 * kRowWarps + 32;  // row warps + the producer warp
 constexpr int kBoxW = kStageBoxW;            // TMA box: source elements per row copy
 constexpr int kHMax = kStageBoxH;            // TMA box: rows per staged plane
-constexpr int kRing = 32;                    // plane slots (plus the mirror of slot 0)
-constexpr int kMinAhead = 2;                 // slots a walk's window leaves for copies in flight
+constexpr int kRing = 16;                    // plane slots (plus the mirror of slot 0); a power of 2
+constexpr int kMinAhead = 3;                 // slots a walk's window leaves for copies in flight
+static_assert((kRing & (kRing - 1)) == 0, "slot = sequence & (kRing - 1)");
 // a wait on a copy or on another warp that has not ended after this long is
 // an error (the kernel reports kKernErrTimeout and returns)
 constexpr unsigned long long kStageWaitNs = 2000000000ull;
 
-// A walk's staging plan (planning kernel).
+// A walk's staging plan (planning kernel), with the walk itself decoded
+// (job, column corner, output planes) so the staged kernel's warps need no
+// 64-bit divisions to find it.
 struct alignas(16) Plan {
     int staged;    // 1: the walk's source footprint is staged
     int a, b;      // output plane z reads source planes [z + a, z + b]
@@ -605,22 +599,11 @@ struct alignas(16) Plan {
     int rows;      // staged rows per plane
     int DX, DY;    // box column / row of frame x = 0 / y = 0
     int nplanes;   // source planes staged for the walk
-    int pad[3];
-};
-
-// Warp 0's copier state: the walk it is planning or copying (the copy
-// frontier) and the ring position of the next copy.
-struct alignas(16) CopyState {
-    int64_t u;        // flattened unit index of the frontier walk (>= total: done)
-    int64_t pfirst;   // buffer z of the frontier walk's first staged plane
-    int loaded;       // the frontier walk's plan is loaded
-    int n;            // planes to copy for the frontier walk (0: not staged)
-    int i;            // next plane of the frontier walk to copy
-    int j;            // job of the frontier walk
-    int rx0, ry0;     // the frontier walk's box corner
-    int last_job;     // job whose tensor map was last acquired
-    uint32_t seq;     // planes copied so far
-    uint32_t slot;    // seq % kRing
+    int interior;  // 1: every sample of the walk is inside (no range tests)
+    int j;         // job
+    int ox, oy;    // global output voxel of the column's corner
+    int z0, z1;    // output planes [z0, z1)
+    int pad;
 };
 
 template <typename T, int G>
@@ -632,11 +615,14 @@ struct TGeom {
     static constexpr int PLANE_B = kHMax * ROW_B;
     static constexpr int RING_B = (kRing + 1) * PLANE_B;
     static constexpr int NBAR = 2 * kRing;        // full[kRing], empty[kRing]
+    // ring, barriers, then the weight tables: W[G] (float4) and W2[G][2]
+    // (float4 pairs (w0, w0, w1, w1), (w2, w2, w3, w3)), then the row warps'
+    // nodes (two float4 per y-contracted node: the interior walks keep them
+    // as duplicated pairs)
     static constexpr size_t smem_bytes =
-        128 + (size_t)RING_B + 8 * NBAR + sizeof(CopyState) + sizeof(float4) * (size_t)(G + kRowWarps * NRW);
+        128 + (size_t)RING_B + 8 * NBAR + sizeof(float4) * (size_t)(3 * G + kRowWarps * 2 * NRW);
     static_assert(PLANE_B % 128 == 0, "TMA destinations are 128-byte aligned");
-    static_assert((8 * NBAR) % 16 == 0 && sizeof(Plan) % 16 == 0 && sizeof(CopyState) % 16 == 0,
-                  "the weight table is float4-aligned");
+    static_assert((8 * NBAR) % 16 == 0 && sizeof(Plan) % 16 == 0, "the weight tables are float4-aligned");
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
@@ -674,26 +660,40 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
     return ok != 0;
 }
 
-// Has the phase of parity `parity` of the mbarrier at `a` completed?  Never
-// suspends the thread (try_wait may suspend it for a while when the phase is
-// incomplete; the copier must not be held up that way).
-__device__ __forceinline__ bool mbar_test(uint32_t a, uint32_t parity)
+// try_wait with a suspend-time hint: a thread whose phase is not complete
+// sleeps until it completes or about hint_ns pass, instead of returning at
+// once, so a waiting warp takes almost no issue slots from the other warps
+// of its SM sub-partition.
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t a, uint32_t parity, uint32_t hint_ns)
 {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
 
+// The producer's wait for a free slot (bounded like mbar_wait_slow): it
+// sleeps between tries, since it has nothing else to do meanwhile.
+__device__ __forceinline__ bool mbar_wait_producer(uint32_t a, uint32_t parity, const volatile int *abort)
+{
+    if (mbar_try(a, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_try_sleep(a, parity, 20000u)) return true;
+        if (*abort || globaltimer_ns() - t0 > kStageWaitNs) return false;
+    }
+}
+
 // Waits for the phase of parity `parity` of the mbarrier at `a`; gives up
 // (false) after kStageWaitNs, or early once another warp has given up
-// (*abort set) unless `drain`.
-__device__ __noinline__ bool mbar_wait_slow(uint32_t a, uint32_t parity, const volatile int *abort, bool drain)
+// (*abort set) unless `drain`.  Inlined: a call would make the hot loops
+// keep registers on the stack around it.
+__device__ __forceinline__ bool mbar_wait_slow(uint32_t a, uint32_t parity, const volatile int *abort, bool drain)
 {
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned i = 1;; ++i) {
@@ -724,8 +724,8 @@ struct TSmem {
     unsigned char *base;  // 128-byte aligned start of the ring
     uint32_t sring;       // shared-window address of slot 0
     uint32_t sfull;       // shared-window address of full[0] (8 bytes each); empty[s] = full[s] + 8 kRing
-    CopyState *cs;        // warp 0's copier state
     float4 *W;            // B-spline weights at t = i / G
+    float4 *W2;           // the same as duplicated pairs: W2[2i] = (w0, w0, w1, w1), W2[2i+1] = (w2, w2, w3, w3)
     float4 *Rw;           // per row warp: y-contracted nodes of its row
     int *abort;           // set by a warp that gave up waiting
 };
@@ -814,8 +814,9 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     if (b - a + 1 + kMinAhead > kRing) return P;
     const int64_t ry0 = w.Oy - J.src_o[1] + fy0;
     const int64_t p0 = w.z0 + a - J.src_o[2], p1 = w.z1 - 1 + b - J.src_o[2];
-    const int64_t lim = (int64_t)1 << 30;  // TMA coordinates are int32
+    const int64_t lim = (int64_t)1 << 30;  // TMA coordinates and the plan's coordinates are int32
     if (rx0 < -lim || rx0 > lim || ry0 < -lim || ry0 + rows > lim || p0 < -lim || p1 > lim) return P;
+    if (w.Ox > lim || w.Oy > lim || w.z1 > lim) return P;
     P.staged = 1;
     P.a = a;
     P.b = b;
@@ -825,94 +826,103 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     P.DX = (int)(w.Ox - J.src_o[0] - rx0);
     P.DY = -fy0;
     P.nplanes = (int)(w.z1 - w.z0) + b - a;
+    P.j = w.j;
+    P.ox = (int)w.Ox;
+    P.oy = (int)w.Oy;
+    P.z0 = (int)w.z0;
+    P.z1 = (int)w.z1;
+    // interior: the unit lies wholly inside the output region, its voxel
+    // pairs can be stored as one word each, and every sample q (with the
+    // margin) has 0 <= floor(q) and floor(q) + 1 <= sz - 1 inside both the
+    // subject volume and the source buffer, so no range test can fail
+    const int64_t pe[3] = {w.Ox + kTBX - 1, w.Oy + kTBY - 1, w.z1 - 1};
+    const int64_t ps[3] = {w.Ox, w.Oy, w.z0};
+    bool in = w.Ox + kTBX <= J.out_o[0] + J.out_n[0] && w.Oy + kTBY <= J.out_o[1] + J.out_n[1];
+    in = in && ((uintptr_t)J.dst) % (2 * sizeof(T)) == 0 && J.dst_py % 2 == 0 && J.dst_pz % 2 == 0;
+    for (int ax = 0; ax < 3; ++ax) {
+        const double lo = (double)ps[ax] + (double)mn[ax] - (double)e;
+        const double hi = (double)pe[ax] + (double)mx[ax] + (double)e;
+        const double vlo = (double)max((int64_t)0, J.src_o[ax]);
+        const double vhi = (double)min(J.glob[ax] - 1, J.src_o[ax] + J.src_n[ax] - 1);
+        in = in && lo >= vlo && hi < vhi;
+    }
+    P.interior = in ? 1 : 0;
     return P;
 }
 
-// Warp 0's copier role, never blocking: issues plane copies of the CTA's
-// staged walks (plans from the planning kernel), in ring order, for as long
-// as ring slots are free (released by every warp).  Called by warp 0 between
-// its planes and while it waits.
+// The producer (lane 0 of the producer warp): copies every source plane of
+// the CTA's staged walks, in walk order, into the ring; plane sequence s
+// goes to slot s & (kRing - 1).  Before it reuses a slot it waits for the
+// slot's "empty" phase: every row warp's reads of the slot's previous plane
+// happen before its arrival there (a release), which the wait observes (an
+// acquire) before the asynchronous write.  seq returns the number of planes
+// issued; false if a wait gave up (or another warp did).
 template <typename T, int G>
-__device__ void copy_ahead(const RJob *__restrict__ jobs, int njobs, int64_t total, const Plan *__restrict__ plans,
-                           const TSmem &S)
+__device__ bool produce(const RJob *__restrict__ jobs, int njobs, int64_t total, const Plan *__restrict__ plans,
+                        const TSmem &S, uint32_t &seq)
 {
     using Gm = TGeom<T, G>;
-    const int lane = threadIdx.x & 31;
-    CopyState &C = *S.cs;
-    // bounded work per call: a ring's worth of copies and a few walks
-    for (int step = 0; step < kRing + 8; ++step) {
-        __syncwarp();  // lane 0's last update of C is visible
-        const int64_t u = C.u;
-        if (u >= total) return;
-        if (!C.loaded) {
-            const Plan P = plans[u];
-            const int j = find_job(jobs, njobs, u);
-            const RJob &J = jobs[j];
-            const int64_t lu = u - J.brick_begin;
-            const int64_t z0 = J.out_o[2] + (lu % J.bricks[2]) * J.zs;
-            if (P.staged && j != C.last_job)  // the descriptor was written by a copy
-                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
-            __syncwarp();
-            if (lane == 0) {
-                C.n = P.staged ? P.nplanes : 0;
-                C.i = 0;
-                C.j = j;
-                C.rx0 = P.rx0;
-                C.ry0 = P.ry0;
-                C.pfirst = z0 + P.a - J.src_o[2];
-                if (P.staged) C.last_job = j;
-                C.loaded = 1;
-            }
-            continue;
+    seq = 0;
+    int last_job = -1;
+    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+        const Plan P = plans[u];
+        if (!P.staged) continue;
+        const RJob &J = jobs[P.j];
+        if (P.j != last_job) {  // the descriptor was written by a copy
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
+            last_job = P.j;
         }
-        const int i = C.i;
-        if (i >= C.n) {  // the frontier walk is copied: on to the next
-            __syncwarp();
-            if (lane == 0) {
-                C.u = u + gridDim.x;
-                C.loaded = 0;
-            }
-            continue;
-        }
-        const uint32_t seq = C.seq, slot = C.slot;
-        const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
-        if (seq >= (uint32_t)kRing && !mbar_test(empty, (seq / kRing - 1u) & 1u)) return;
-        const RJob &J = jobs[C.j];
-        const int rx0 = C.rx0, ry0 = C.ry0;
-        const int pz = (int)(C.pfirst + i);
-        if (lane == 0) {
-            // every warp's reads of the slot's previous plane happen before its
-            // arrival on the slot's empty barrier (a release), which this warp
-            // observed (an acquire) before issuing the asynchronous write
+        const int pfirst = (int)((int64_t)P.z0 + P.a - J.src_o[2]);
+        for (int i = 0; i < P.nplanes; ++i, ++seq) {
+            const uint32_t slot = seq & (uint32_t)(kRing - 1);
+            const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
+            if (seq >= (uint32_t)kRing && !mbar_wait_producer(empty, (seq / kRing - 1u) & 1u, S.abort))
+                return false;
             mbar_expect_tx(full, (uint32_t)(slot == 0 ? 2 : 1) * (uint32_t)Gm::PLANE_B);
             const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B;
-            tma_plane(d, &J.tmap, rx0, ry0, pz, full);
-            if (slot == 0) tma_plane(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, rx0, ry0, pz, full);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            C.i = i + 1;
-            C.seq = seq + 1u;
-            C.slot = slot + 1u == (uint32_t)kRing ? 0u : slot + 1u;
+            tma_plane(d, &J.tmap, P.rx0, P.ry0, pfirst + i, full);
+            if (slot == 0) tma_plane(d + (uint32_t)(kRing * Gm::PLANE_B), &J.tmap, P.rx0, P.ry0, pfirst + i, full);
         }
     }
+    return true;
 }
 
-// Waits for the phase of parity `parity` of the mbarrier at `a`; warp 0
-// keeps its copier role going meanwhile.  false if the wait gave up.
-template <typename T, int G>
-__device__ __forceinline__ bool wait_copying(uint32_t a, uint32_t parity, bool copier, const RJob *__restrict__ jobs,
-                                             int njobs, int64_t total, const Plan *__restrict__ plans, const TSmem &S)
+// The producer on its way out: every copy it issued has landed before the
+// CTA exits (the row warps waited for all of them unless a wait gave up;
+// bounded waits).
+__device__ void drain_copies(const TSmem &S, uint32_t seq)
 {
-    if (!copier) return mbar_try(a, parity) || mbar_wait_slow(a, parity, S.abort, false);
-    if (mbar_test(a, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (unsigned n = 1;; ++n) {
-        copy_ahead<T, G>(jobs, njobs, total, plans, S);
-        if (mbar_test(a, parity)) return true;
-        if ((n & 15u) == 0 && (*reinterpret_cast<volatile int *>(S.abort) || globaltimer_ns() - t0 > kStageWaitNs))
-            return false;
+    const uint32_t n0 = seq > (uint32_t)kRing ? seq - kRing : 0u;
+    for (uint32_t n = n0; n < seq; ++n)
+        if (!mbar_try(S.sfull + 8u * (n % kRing), (n / kRing) & 1u))
+            mbar_wait_slow(S.sfull + 8u * (n % kRing), (n / kRing) & 1u, S.abort, true);
+}
+
+// A row warp's place in the ring: the next plane sequence to wait for and
+// the next to release.  A walk's planes are consecutive sequences, so at
+// the start of a walk rseq = wseq = the sequence of its first plane.
+struct RingPos {
+    uint32_t wseq, rseq;
+};
+
+// Waits (bounded) for the planes before sequence `need`; false if a wait
+// gave up.  Every lane waits; the outcome is made uniform across the warp.
+__device__ __forceinline__ bool wait_planes(const TSmem &S, RingPos &R, uint32_t need)
+{
+    for (; R.wseq < need; ++R.wseq) {
+        const bool ok = mbar_wait(S.sfull + 8u * (R.wseq & (uint32_t)(kRing - 1)), (R.wseq / kRing) & 1u, S.abort);
+        if (!__all_sync(0xffffffffu, ok)) return false;
     }
+    return true;
+}
+
+// Releases the oldest plane the warp holds: every lane arrives on the slot's
+// "empty" barrier (32 arrivals per row warp), each arrival a release of that
+// lane's reads of the plane.
+__device__ __forceinline__ void release_plane(const TSmem &S, RingPos &R)
+{
+    mbar_arrive(S.sfull + 8u * (kRing + (R.rseq & (uint32_t)(kRing - 1))));
+    ++R.rseq;
 }
 
 // The row warps' state of one cell layer (uniform across the warp except
@@ -1029,26 +1039,139 @@ __device__ __forceinline__ void plane_positions(const RowLayer &L, float4 wz, fl
     pz = fma2(w0, L.P[0][2], fma2(w1, L.P[1][2], fma2(w2, L.P[2][2], fma2(w3, L.P[3][2], f2(0.f, 0.f)))));
 }
 
-// Offset (from the ring base) of the (x, y, z) = floor tap of a staged
-// sample, from the magic-floor bit patterns; cz maps a tap plane to its
-// slot (the ring wrap is one unsigned min); clamped so that all 8 taps stay
-// in the ring.
-template <typename T>
-__device__ __forceinline__ uint32_t staged_off(uint32_t kxy, uint32_t omax, uint32_t cz, float mx, float my, float mz)
-{
-    constexpr uint32_t ROW_B = kBoxW * sizeof(T), PLANE_B = kHMax * ROW_B;
-    const uint32_t t = __float_as_uint(mz) + cz;  // slot, or slot + kRing past the wrap
-    const uint32_t slot = min(t, t - (uint32_t)kRing);
-    const uint32_t o = slot * PLANE_B + __float_as_uint(my) * ROW_B + __float_as_uint(mx) * (uint32_t)sizeof(T) + kxy;
-    return min(o, omax);
-}
-
 // Magic float 2^23 + v of the staged voxel at offset o.
 template <typename T>
 __device__ __forceinline__ float smag(const unsigned char *sm, uint32_t o)
 {
     return __int_as_float(0x4B000000 | (int)(uint32_t)*reinterpret_cast<const T *>(sm + o));
 }
+
+// Offset (from the ring base) of the (x, y, z) = floor tap of a staged
+// sample, from the magic-floor bit patterns; cz maps a tap plane to its
+// plane sequence (mod kRing: the slot); clamped so that all 8 taps stay in
+// the ring.
+template <typename T>
+__device__ __forceinline__ uint32_t staged_off(uint32_t kxy, uint32_t omax, uint32_t cz, float mx, float my, float mz)
+{
+    constexpr uint32_t ROW_B = kBoxW * sizeof(T), PLANE_B = kHMax * ROW_B;
+    const uint32_t slot = (__float_as_uint(mz) + cz) & (uint32_t)(kRing - 1);
+    const uint32_t o = slot * PLANE_B + __float_as_uint(my) * ROW_B + __float_as_uint(mx) * (uint32_t)sizeof(T) + kxy;
+    return min(o, omax);
+}
+
+// cz of staged_off for the cell layer with frame origin Oz of a walk whose
+// first plane (output plane z0 + a) has sequence seq0: the source plane
+// Oz + iz has sequence seq0 + (Oz + iz) - (z0 + a), and the magic floor's
+// bit pattern of iz is kMagicBits + iz (2^32 wrap arithmetic).
+__device__ __forceinline__ uint32_t layer_cz(uint32_t seq0, int64_t Oz, int64_t z0, int a)
+{
+    return seq0 + (uint32_t)(Oz - z0) - (uint32_t)a - (uint32_t)kMagicBits;
+}
+
+// A voxel pair of an interior walk from the staged planes, in three steps
+// so that a plane's address arithmetic can overlap the previous plane's
+// loads: positions as (voxel 0, voxel 1) pairs per axis give the fractions
+// and the two floor taps' addresses (prep), the eight taps of both voxels
+// are loaded (taps), and the trilinear value is rounded and packed
+// (finish).  No range tests: every tap is inside the staged window.  The
+// same floors, fractions, taps and trilinear arithmetic as pair_staged.
+struct PairPrep {
+    float2 fx, fy, fz;
+    const unsigned char *p0, *p1;  // floor taps of voxel 0 / 1 in the ring
+};
+
+template <typename T>
+__device__ __forceinline__ PairPrep prep_pair(const unsigned char *sm, uint32_t kxy, uint32_t omax, uint32_t cz,
+                                              float2 px, float2 py, float2 pz)
+{
+    const float2 MM = f2(kMagic, kMagic);
+    const float2 mx = __fadd2_rd(px, MM), my = __fadd2_rd(py, MM), mz = __fadd2_rd(pz, MM);
+    PairPrep q;
+    q.fx = sub2(px, sub2(mx, MM));
+    q.fy = sub2(py, sub2(my, MM));
+    q.fz = sub2(pz, sub2(mz, MM));
+    q.p0 = sm + staged_off<T>(kxy, omax, cz, mx.x, my.x, mz.x);
+    q.p1 = sm + staged_off<T>(kxy, omax, cz, mx.y, my.y, mz.y);
+    return q;
+}
+
+// The eight taps of both voxels as magic floats (2^23 + v): constant row,
+// plane and element offsets from each voxel's floor tap.
+template <typename T>
+__device__ __forceinline__ void taps_pair(const PairPrep &q, float2 (&lo)[4], float2 (&hi)[4])
+{
+    constexpr int ES = sizeof(T), ROW_B = kBoxW * ES, PLANE_B = kHMax * ROW_B;
+    constexpr int rofs[4] = {0, ROW_B, PLANE_B, PLANE_B + ROW_B};
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        lo[r] = f2(smag<T>(q.p0 + rofs[r], 0), smag<T>(q.p1 + rofs[r], 0));
+        hi[r] = f2(smag<T>(q.p0 + rofs[r] + ES, 0), smag<T>(q.p1 + rofs[r] + ES, 0));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ uint32_t finish_pair(const PairPrep &q, const float2 (&lo)[4], const float2 (&hi)[4])
+{
+    const float2 t = out_pair<T, true>(trilerp2(lo, hi, q.fx, q.fy, q.fz));
+    return pack_pair<T>(__float_as_uint(t.x), __float_as_uint(t.y));
+}
+
+// Cell-layer set-up of row warp y of an interior walk: the y contraction of
+// the row's nodes into Rw, then the lane's x contraction into position pairs
+// per node layer c: PX[c] = (x of voxel 0, x of voxel 1), PY[c], PZ[c]
+// likewise.  Same operations and order as row_layer (the other walks), so a
+// voxel's position does not depend on which path sampled it.
+template <typename T, int G>
+__device__ __forceinline__ void layer_positions(const RJob &J, int64_t Ox, int64_t Oy, int64_t Oz, int y,
+                                                const float4 *W, float4 *Rw, const float4 (&wx)[2], float2 (&PX)[4],
+                                                float2 (&PY)[4], float2 (&PZ)[4])
+{
+    using Gm = TGeom<T, G>;
+    const int lane = threadIdx.x & 31;
+    const int64_t c0[3] = {Ox / G, Oy / G, Oz / G};
+    const int yy = (int)(Oy - c0[1] * G) + y;
+    const int cyb = yy / G;
+    const float4 wy = W[yy % G];
+    __syncwarp();  // every lane is done with the previous layer's Rw
+    for (int i = lane; i < Gm::NRW; i += 32) {
+        const int c = i / Gm::NX, nx = i % Gm::NX;
+        const int64_t gx = min(c0[0] + nx, J.gsz[0] - 1), gz = min(c0[2] + c, J.gsz[2] - 1);
+        const float ox = (float)((gx - 1) * G - Ox), oz = (float)((gz - 1) * G - Oz);
+        float4 v[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int64_t gy = min(c0[1] + cyb + b, J.gsz[1] - 1);
+            const float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
+            v[b] = make_float4(d.x + ox, d.y + (float)((gy - 1) * G - Oy), d.z + oz, 0.f);
+        }
+        const float rx = fmaf(wy.x, v[0].x, fmaf(wy.y, v[1].x, fmaf(wy.z, v[2].x, wy.w * v[3].x)));
+        const float ry = fmaf(wy.x, v[0].y, fmaf(wy.y, v[1].y, fmaf(wy.z, v[2].y, wy.w * v[3].y)));
+        const float rz = fmaf(wy.x, v[0].z, fmaf(wy.y, v[1].z, fmaf(wy.z, v[2].z, wy.w * v[3].z)));
+        // duplicated pairs: (x, x, y, y), (z, z, -, -) are FP32x2 operands as loaded
+        Rw[2 * i] = make_float4(rx, rx, ry, ry);
+        Rw[2 * i + 1] = make_float4(rz, rz, 0.f, 0.f);
+    }
+    __syncwarp();
+    const int xn = (2 * lane) / G;
+    float2 w[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) w[a] = f2((&wx[0].x)[a], (&wx[1].x)[a]);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float2 px = f2(0.f, 0.f), py = px, pz = px;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const float4 n = Rw[2 * (c * Gm::NX + xn + a)], m = Rw[2 * (c * Gm::NX + xn + a) + 1];
+            px = fma2(w[a], f2(n.x, n.y), px);
+            py = fma2(w[a], f2(n.z, n.w), py);
+            pz = fma2(w[a], f2(m.x, m.y), pz);
+        }
+        PX[c] = px;
+        PY[c] = py;
+        PZ[c] = pz;
+    }
+}
+
 
 // A voxel pair sampled from the staged planes.  CHECKED applies the
 // reference's range rule per voxel (0 <= q <= sz-1, else 0) and clamps floor(q)
@@ -1093,9 +1216,9 @@ __device__ __forceinline__ uint32_t pair_staged(const unsigned char *sm, uint32_
     constexpr uint32_t rofs[4] = {0u, ROW_B, PLANE_B, PLANE_B + ROW_B};
     float2 lo[4], hi[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        lo[r] = f2(smag<T>(sm, o0 + rofs[r]), smag<T>(sm, o1 + rofs[r]));
-        hi[r] = f2(smag<T>(sm, o0 + rofs[r] + ES), smag<T>(sm, o1 + rofs[r] + ES));
+    for (int r = 0; r < 4; ++r) {  // constant offsets from the floor taps' addresses
+        lo[r] = f2(smag<T>(sm + o0 + rofs[r], 0), smag<T>(sm + o1 + rofs[r], 0));
+        hi[r] = f2(smag<T>(sm + o0 + rofs[r] + ES, 0), smag<T>(sm + o1 + rofs[r] + ES, 0));
     }
     const float2 t = out_pair<T, true>(trilerp2(lo, hi, f2(f0.x, f1.x), f2(f0.y, f1.y), fz));
     if (CHECKED)  // a rejected voxel writes 0: the bits of 2^23 have zero low bits
@@ -1147,96 +1270,158 @@ __device__ __forceinline__ void gathered_pair(float2 p0, float2 p1, float2 pz2, 
     }
 }
 
-// The staged kernel's warps: every walk of the CTA, one output row per warp
-// (warp 0 also copies); walks that could not be planned are skipped (the
-// gather kernel takes them).  Returns false if a wait gave up.
+// Positions of a voxel pair on a plane: sum over node layers c of the z
+// weight pairs W2 times the layer's x/y-contracted position pairs (the
+// order of row_layer's plane_positions, so both paths agree bit for bit).
+__device__ __forceinline__ void pair_positions(const float2 (&w)[4], const float2 (&PX)[4], const float2 (&PY)[4],
+                                               const float2 (&PZ)[4], float2 &px, float2 &py, float2 &pz)
+{
+    const float2 Z2 = f2(0.f, 0.f);
+    px = fma2(w[0], PX[0], fma2(w[1], PX[1], fma2(w[2], PX[2], fma2(w[3], PX[3], Z2))));
+    py = fma2(w[0], PY[0], fma2(w[1], PY[1], fma2(w[2], PY[2], fma2(w[3], PY[3], Z2))));
+    pz = fma2(w[0], PZ[0], fma2(w[1], PZ[1], fma2(w[2], PZ[2], fma2(w[3], PZ[3], Z2))));
+}
+
+// Row warp y's part of an interior walk (every sample inside: no range
+// tests, whole rows, paired stores): rows y + k kRowWarps (k < kRowsPerWarp),
+// whose voxel pairs are independent work for the lane.  Per output plane z
+// it waits for the planes up to z + b, samples, stores, and releases plane
+// z + a, which no later plane of the walk reads.  false if a wait gave up.
 template <typename T, int G>
-__device__ bool rows_staged(const RJob *__restrict__ jobs, int njobs, int64_t total, const Plan *__restrict__ plans,
-                            const TSmem &S)
+__device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
+                              const float4 (&wx)[2], RingPos &R)
 {
     using Gm = TGeom<T, G>;
+    constexpr int NR = kRowsPerWarp;
     const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool copier = y == 0;
-    const int x = 2 * lane;
-    float4 *Rw = S.Rw + y * Gm::NRW;
-    const float4 wx[2] = {S.W[x % G], S.W[(x + 1) % G]};
-    const unsigned char *sm = S.base;
-    uint32_t wslot = 0, wpar = 0;  // next ring sequence to wait for: slot, phase parity
-    uint32_t rslot = 0;            // slot of the next sequence to release
-    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
-        const Plan P = plans[u];
-        if (!P.staged) continue;
-        const Walk w = walk_of(jobs, njobs, u);
-        const RJob &J = jobs[w.j];
-        const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
-        const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;
-        const int64_t dst_pz = J.dst_pz;
-        // a voxel pair (even x) can be written as one 2-element store
-        const bool pair_ok =
-            (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
-        T *drow = static_cast<T *>(J.dst) +
-                  ((w.z0 - J.out_o[2]) * dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
-        // frame (0, 0) in slot 0 minus the magic-float bias of the floor bit
-        // patterns (2^32 wrap arithmetic)
-        const uint32_t kxy =
-            (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
-        const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
-        const int Wn = P.b - P.a + 1;  // planes of a window
-        int waited = 0, need = Wn;     // sequences of this walk waited for / needed by the next plane
-        for (int64_t zf = w.z0; zf < w.z1;) {
-            const int64_t ze = min(w.z1, (zf / G + 1) * G);
-            const int64_t Oz = (zf / G) * G;
-            const int zoff = (int)(zf - Oz), zn = (int)(ze - zf);
-            RowLayer L;
-            if (rowv) row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, S.W, Rw, wx, L);
-            for (int pz = zoff; pz < zoff + zn; ++pz) {  // frame z of the plane
-                while (waited < need) {
-                    if (!wait_copying<T, G>(S.sfull + 8u * wslot, wpar, copier, jobs, njobs, total, plans, S))
-                        return false;
-                    ++waited;
-                    if (++wslot == (uint32_t)kRing) {
-                        wslot = 0;
-                        wpar ^= 1u;
-                    }
-                }
-                if (rowv) {
-                    float2 p0, p1, pz2;
-                    plane_positions(L, S.W[pz], p0, p1, pz2);
-                    const float fz = (float)pz;
-                    // slot of a tap plane: (tap plane - window start) + slot(window start)
-                    const uint32_t cz = rslot - (uint32_t)(pz + P.a) - (uint32_t)kMagicBits;
-                    if (L.row_fast && fz >= L.zlo && fz < L.zhi) {
-                        const Frame unused = {};
-                        const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
-                        const uint32_t v = pair_staged<T, false>(sm, kxy, omax, cz, p0, p1, pz2, unused, wl, wh, 2);
-                        store_packed<T>(drow + x, v, pair_ok, 2);
-                    } else if (x < xe) {
-                        const int64_t O[3] = {w.Ox, w.Oy, Oz};
-                        const Frame frame = make_frame(J, O);
-                        const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(pz + P.a)};
-                        const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
-                                             (float)(pz + P.b - 1)};
-                        const uint32_t v = pair_staged<T, true>(sm, kxy, omax, cz, p0, p1, pz2, frame, wl, wh, xe - x);
-                        store_packed<T>(drow + x, v, pair_ok, xe - x);
-                    }
-                }
-                drow += dst_pz;
-                // the window start is not read by later planes
-                __syncwarp();
-                if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
-                if (++rslot == (uint32_t)kRing) rslot = 0;
-                ++need;
-                if (copier) copy_ahead<T, G>(jobs, njobs, total, plans, S);
+    const uint32_t seq0 = R.rseq;   // sequence of the walk's first plane
+    const uint32_t Wn = (uint32_t)(P.b - P.a + 1);  // planes of a window
+    T *dp = static_cast<T *>(J.dst) +
+            ((w.z0 - J.out_o[2]) * J.dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0])) + 2 * lane;
+    const int64_t dpz = J.dst_pz, drow2 = kRowWarps * J.dst_py;
+    // frame (0, 0) in slot 0 minus the magic-float bias of the floor bit
+    // patterns (2^32 wrap arithmetic)
+    const uint32_t kxy =
+        (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
+    const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
+    for (int64_t zf = w.z0; zf < w.z1;) {
+        const int64_t ze = min(w.z1, (zf / G + 1) * G);
+        const int64_t Oz = (zf / G) * G;
+        const int zoff = (int)(zf - Oz), zend = (int)(ze - Oz);
+        float2 PX[NR][4], PY[NR][4], PZ[NR][4];
+#pragma unroll
+        for (int k = 0; k < NR; ++k)
+            layer_positions<T, G>(J, w.Ox, w.Oy, Oz, y + k * kRowWarps, S.W, Rw, wx, PX[k], PY[k], PZ[k]);
+        const uint32_t cz = layer_cz(seq0, Oz, w.z0, P.a);
+        // the fractions and tap addresses of plane pz are computed during
+        // plane pz - 1 (they need no staged data), so that their arithmetic
+        // overlaps the previous plane's loads
+        auto prep = [&](int p, PairPrep (&q)[NR]) {
+            const float4 wa = S.W2[2 * p], wb = S.W2[2 * p + 1];
+            const float2 wz[4] = {f2(wa.x, wa.y), f2(wa.z, wa.w), f2(wb.x, wb.y), f2(wb.z, wb.w)};
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                float2 px, py, pz;
+                pair_positions(wz, PX[k], PY[k], PZ[k], px, py, pz);
+                q[k] = prep_pair<T>(S.base, kxy, omax, cz, px, py, pz);
             }
-            zf = ze;
+        };
+        PairPrep q[NR];
+        prep(zoff, q);
+        // sequence past the last plane output plane Oz + pz reads
+        uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
+        for (int pz = zoff; pz < zend; ++pz, ++need) {
+            if (!wait_planes(S, R, need)) return false;
+            float2 lo[NR][4], hi[NR][4];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) taps_pair<T>(q[k], lo[k], hi[k]);
+            PairPrep nq[NR];
+            prep(min(pz + 1, G - 1), nq);  // (the last plane's is not used)
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                const uint32_t v = finish_pair<T>(q[k], lo[k], hi[k]);
+                if (sizeof(T) == 2) *reinterpret_cast<uint32_t *>(dp + k * drow2) = v;
+                else *reinterpret_cast<uint16_t *>(dp + k * drow2) = (uint16_t)v;
+                q[k] = nq[k];
+            }
+            dp += dpz;
+            release_plane(S, R);
         }
-        // the rest of the last window
-        __syncwarp();
-        for (int i = 1; i < Wn; ++i) {
-            if (lane == 0) mbar_arrive(S.sfull + 8u * (kRing + rslot));
-            if (++rslot == (uint32_t)kRing) rslot = 0;
-        }
+        zf = ze;
     }
+    for (uint32_t i = 1; i < Wn; ++i) release_plane(S, R);  // the rest of the last window
+    return true;
+}
+
+// Row warp y's part of any other staged walk (rows y and y + kRowWarps):
+// the layer's sample hull decides per row and plane between the unchecked
+// staged sample and the checked one (the reference's range rule per voxel,
+// taps clamped into the staged window).  false if a wait gave up.
+template <typename T, int G>
+__device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
+                             const float4 (&wx)[2], RingPos &R)
+{
+    using Gm = TGeom<T, G>;
+    const int lane = threadIdx.x & 31;
+    const int x = 2 * lane;
+    const uint32_t seq0 = R.rseq;
+    const uint32_t Wn = (uint32_t)(P.b - P.a + 1);
+    const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
+    const int64_t dst_pz = J.dst_pz;
+    // a voxel pair (even x) can be written as one 2-element store
+    const bool pair_ok = (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
+    const uint32_t kxy =
+        (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
+    const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
+    const int y0 = threadIdx.x >> 5;
+    T *drow = static_cast<T *>(J.dst) +
+              ((w.z0 - J.out_o[2]) * dst_pz + (w.Oy + y0 - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
+    const int64_t drow2 = kRowWarps * J.dst_py;
+    for (int64_t zf = w.z0; zf < w.z1;) {
+        const int64_t ze = min(w.z1, (zf / G + 1) * G);
+        const int64_t Oz = (zf / G) * G;
+        const int zoff = (int)(zf - Oz), zn = (int)(ze - zf);
+        RowLayer L[kRowsPerWarp];
+        bool rowv[kRowsPerWarp];
+#pragma unroll
+        for (int k = 0; k < kRowsPerWarp; ++k) {
+            const int y = y0 + k * kRowWarps;
+            rowv[k] = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;
+            if (rowv[k]) row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, S.W, Rw, wx, L[k]);
+        }
+        const uint32_t cz = layer_cz(seq0, Oz, w.z0, P.a);
+        uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
+        for (int pz = zoff; pz < zoff + zn; ++pz, ++need) {  // frame z of the plane
+            if (!wait_planes(S, R, need)) return false;
+#pragma unroll
+            for (int k = 0; k < kRowsPerWarp; ++k) {
+                if (!rowv[k]) continue;
+                T *dr = drow + k * drow2;
+                float2 p0, p1, pz2;
+                plane_positions(L[k], S.W[pz], p0, p1, pz2);
+                const float fz = (float)pz;
+                if (L[k].row_fast && fz >= L[k].zlo && fz < L[k].zhi) {
+                    const Frame unused = {};
+                    const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
+                    const uint32_t v = pair_staged<T, false>(S.base, kxy, omax, cz, p0, p1, pz2, unused, wl, wh, 2);
+                    store_packed<T>(dr + x, v, pair_ok, 2);
+                } else if (x < xe) {
+                    const int64_t O[3] = {w.Ox, w.Oy, Oz};
+                    const Frame frame = make_frame(J, O);
+                    const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(pz + P.a)};
+                    const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
+                                         (float)(pz + P.b - 1)};
+                    const uint32_t v =
+                        pair_staged<T, true>(S.base, kxy, omax, cz, p0, p1, pz2, frame, wl, wh, xe - x);
+                    store_packed<T>(dr + x, v, pair_ok, xe - x);
+                }
+            }
+            drow += dst_pz;
+            release_plane(S, R);  // the window start is not read by later planes
+        }
+        zf = ze;
+    }
+    for (uint32_t i = 1; i < Wn; ++i) release_plane(S, R);  // the rest of the last window
     return true;
 }
 
@@ -1282,17 +1467,6 @@ __device__ void rows_gather(const RJob *__restrict__ jobs, int njobs, int64_t u,
         }
         zf = ze;
     }
-}
-
-// Warp 0, on its way out: every copy it issued lands before the CTA exits
-// (all of them have been waited for unless a wait gave up; bounded waits).
-__device__ void drain_copies(const TSmem &S)
-{
-    const uint32_t seq = S.cs->seq;
-    const uint32_t n0 = seq > (uint32_t)kRing ? seq - kRing : 0u;
-    for (uint32_t n = n0; n < seq; ++n)
-        if (!mbar_try(S.sfull + 8u * (n % kRing), (n / kRing) & 1u))
-            mbar_wait_slow(S.sfull + 8u * (n % kRing), (n / kRing) & 1u, S.abort, true);
 }
 
 // ---------------------------------------------------------------- affine
@@ -1448,49 +1622,76 @@ __global__ void __launch_bounds__(256) k_tps_plan(const RJob *__restrict__ jobs,
 // TPS units whose source footprint is staged by TMA (trilinear), with the
 // plans of k_tps_plan; units without a staged plan are left to k_tps_gather.
 template <typename T, int G>
-__global__ void __launch_bounds__(kTpsThreads, 1) k_tps_staged(const RJob *__restrict__ jobs, int njobs,
-                                                                int64_t total_units, const Plan *__restrict__ plans,
-                                                                int *err)
+__global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__restrict__ jobs, int njobs,
+                                                                   int64_t total_units, const Plan *__restrict__ plans,
+                                                                   int *err)
 {
     using Gm = TGeom<T, G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int abort_sh;
     // ring slots first, on a 128-byte boundary (TMA destinations), then the
-    // mbarriers, the copier state, the weight table and the warps' node rows
+    // mbarriers, the weight tables and the row warps' node rows
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t pad = (128u - (raw & 127u)) & 127u;
     TSmem S;
     S.base = smem_raw + pad;
     S.sring = raw + pad;
     S.sfull = S.sring + (uint32_t)Gm::RING_B;
-    unsigned char *tail = S.base + Gm::RING_B + 8 * Gm::NBAR;
-    S.cs = reinterpret_cast<CopyState *>(tail);
-    S.W = reinterpret_cast<float4 *>(tail + sizeof(CopyState));
-    S.Rw = S.W + G;
+    S.W = reinterpret_cast<float4 *>(S.base + Gm::RING_B + 8 * Gm::NBAR);
+    S.W2 = S.W + G;
+    S.Rw = S.W2 + 2 * G;
     S.abort = &abort_sh;
     const int tid = threadIdx.x;
-    if (tid < G) S.W[tid] = bspline_w(tid, G);
+    if (tid < G) {
+        const float4 w = bspline_w(tid, G);
+        S.W[tid] = w;
+        S.W2[2 * tid] = make_float4(w.x, w.x, w.y, w.y);
+        S.W2[2 * tid + 1] = make_float4(w.z, w.z, w.w, w.w);
+    }
     if (tid < kRing) {
         mbar_init(S.sfull + 8u * tid, 1);
-        mbar_init(S.sfull + 8u * (kRing + tid), kRowWarps);
+        mbar_init(S.sfull + 8u * (kRing + tid), 32 * kRowWarps);  // every lane of every row warp
     }
     if (tid == 0) {
         abort_sh = 0;
-        CopyState c = {};
-        c.u = blockIdx.x;
-        c.last_job = -1;
-        *S.cs = c;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid < 32) copy_ahead<T, G>(jobs, njobs, total_units, plans, S);
-    const bool ok = rows_staged<T, G>(jobs, njobs, total_units, plans, S);
-    if (!ok) {
-        // the other warps see the flag in their waits and return
-        *reinterpret_cast<volatile int *>(&abort_sh) = 1;
-        if ((tid & 31) == 0 && err) atomicOr(err, kKernErrTimeout);
+    const int warp = tid >> 5, lane = tid & 31;
+    if (warp == kRowWarps) {  // the producer warp: lane 0 issues every copy
+        if (lane == 0) {
+            uint32_t seq = 0;
+            if (!produce<T, G>(jobs, njobs, total_units, plans, S, seq)) {
+                *reinterpret_cast<volatile int *>(&abort_sh) = 1;  // the row warps see it in their waits
+                if (err) atomicOr(err, kKernErrTimeout);
+            }
+            drain_copies(S, seq);
+        }
+        return;
     }
-    if (tid < 32) drain_copies(S);
+    float4 *Rw = S.Rw + warp * 2 * Gm::NRW;
+    const int x = 2 * lane;
+    const float4 wx[2] = {S.W[x % G], S.W[(x + 1) % G]};
+    RingPos R = {0u, 0u};
+    for (int64_t u = blockIdx.x; u < total_units; u += gridDim.x) {
+        const Plan P = plans[u];
+        if (!P.staged) continue;  // the gather kernel takes it
+        Walk w;
+        w.j = P.j;
+        w.Ox = P.ox;
+        w.Oy = P.oy;
+        w.z0 = P.z0;
+        w.z1 = P.z1;
+        const RJob &J = jobs[w.j];
+        const bool ok = P.interior ? walk_interior<T, G>(J, w, P, S, Rw, wx, R)
+                                   : walk_checked<T, G>(J, w, P, S, Rw, wx, R);
+        if (!ok) {
+            // the other warps see the flag in their waits and return
+            *reinterpret_cast<volatile int *>(&abort_sh) = 1;
+            if (lane == 0 && err) atomicOr(err, kKernErrTimeout);
+            return;
+        }
+    }
 }
 
 // TPS units gathered from global memory: the units of fb when it is given
@@ -1501,7 +1702,7 @@ __global__ void __launch_bounds__(kTpsThreads, 1) k_tps_gather(const RJob *__res
 {
     using Gm = TGeom<T, G>;
     __shared__ float4 W[G];
-    __shared__ float4 Rw[kRowWarps * Gm::NRW];
+    __shared__ float4 Rw[kTBY * Gm::NRW];
     const int tid = threadIdx.x;
     if (tid < G) W[tid] = bspline_w(tid, G);
     __syncthreads();
@@ -1551,13 +1752,13 @@ cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
         if (e != cudaSuccess) return e;
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTpsThreads, Gm::smem_bytes);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kStagedThreads, Gm::smem_bytes);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
         int64_t grid = (int64_t)sms * per_sm;
         if (grid > total) grid = total;
         if (grid < 1) grid = 1;
-        k<<<(unsigned)grid, kTpsThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, plans, err);
+        k<<<(unsigned)grid, kStagedThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, plans, err);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
