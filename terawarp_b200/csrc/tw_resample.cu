@@ -554,10 +554,13 @@ __device__ __forceinline__ Clamp make_clamp(const RJob &J, const Frame &f, const
 // planes ahead of the slowest row warp and no row warp waits for another
 // except through the data.  Slot 0 is copied a second time past the last
 // slot, so the z+1 tap of any plane is at a fixed offset.  A slot holds the
-// box densely (row pitch kBoxW).  Units are numbered z-fastest, so the walks
-// of one column (which share their halo planes) and of neighbouring columns
-// (which share halo rows) run at the same time on neighbouring CTAs and meet
-// in L2.  A walk whose box or window does not fit, a nearest-neighbour job,
+// box densely (row pitch kBoxW).  Units are numbered x-fastest, then y,
+// then z, so the walks in flight at one time are a slab of neighbouring
+// columns at the same depth: their boxes overlap in x and y and meet in L2,
+// and each source plane comes from DRAM about once.  (Numbered z-fastest,
+// the walks in flight were a few columns at 16 depths and the y-neighbours'
+// halo rows were fetched again later: 3x the source bytes read from DRAM on
+// a 1024^3 u16 job.)  A walk whose box or window does not fit, a nearest-neighbour job,
 // or a source buffer TMA cannot describe gathers from global memory instead
 // (the gather kernel), with the same positions and the same trilinear
 // arithmetic (trilerp2).
@@ -730,8 +733,9 @@ struct TSmem {
     int *abort;           // set by a warp that gave up waiting
 };
 
-// Job and unit of flattened unit index u (z fastest: consecutive units are
-// the walks of one column).
+// Job and unit of flattened unit index u (x fastest, then y, then z: the
+// units that run at the same time are a compact slab of neighbouring
+// columns at the same depth, whose overlapping source footprints meet in L2).
 struct Walk {
     int j;
     int64_t Ox, Oy, z0, z1;
@@ -743,8 +747,8 @@ __device__ __forceinline__ Walk walk_of(const RJob *jobs, int njobs, int64_t u)
     w.j = find_job(jobs, njobs, u);
     const RJob &J = jobs[w.j];
     const int64_t lu = u - J.brick_begin;
-    const int64_t bz = lu % J.bricks[2], t = lu / J.bricks[2];
-    const int64_t bx = t % J.bricks[0], by = t / J.bricks[0];
+    const int64_t bx = lu % J.bricks[0], t = lu / J.bricks[0];
+    const int64_t by = t % J.bricks[1], bz = t / J.bricks[1];
     w.Ox = J.out_o[0] + bx * kTBX;
     w.Oy = J.out_o[1] + by * kTBY;
     w.z0 = J.out_o[2] + bz * J.zs;
@@ -839,6 +843,7 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     const int64_t ps[3] = {w.Ox, w.Oy, w.z0};
     bool in = w.Ox + kTBX <= J.out_o[0] + J.out_n[0] && w.Oy + kTBY <= J.out_o[1] + J.out_n[1];
     in = in && ((uintptr_t)J.dst) % (2 * sizeof(T)) == 0 && J.dst_py % 2 == 0 && J.dst_pz % 2 == 0;
+    in = in && J.gsz[0] * J.gsz[1] * J.gsz[2] < ((int64_t)1 << 31);  // node indices of interior walks are 32-bit
     for (int ax = 0; ax < 3; ++ax) {
         const double lo = (double)ps[ax] + (double)mn[ax] - (double)e;
         const double hi = (double)pe[ax] + (double)mx[ax] + (double)e;
@@ -1128,21 +1133,26 @@ __device__ __forceinline__ void layer_positions(const RJob &J, int64_t Ox, int64
 {
     using Gm = TGeom<T, G>;
     const int lane = threadIdx.x & 31;
-    const int64_t c0[3] = {Ox / G, Oy / G, Oz / G};
-    const int yy = (int)(Oy - c0[1] * G) + y;
+    // interior walks have int32 coordinates and node indices (the planning
+    // kernel checks the coordinates; node grids stay below 2^31 nodes)
+    const int ox0 = (int)Ox, oy0 = (int)Oy, oz0 = (int)Oz;
+    const int c0[3] = {ox0 / G, oy0 / G, oz0 / G};
+    const int gs0 = (int)J.gsz[0], gs1 = (int)J.gsz[1], gs2 = (int)J.gsz[2];
+    const int yy = oy0 - c0[1] * G + y;
     const int cyb = yy / G;
     const float4 wy = W[yy % G];
     __syncwarp();  // every lane is done with the previous layer's Rw
     for (int i = lane; i < Gm::NRW; i += 32) {
         const int c = i / Gm::NX, nx = i % Gm::NX;
-        const int64_t gx = min(c0[0] + nx, J.gsz[0] - 1), gz = min(c0[2] + c, J.gsz[2] - 1);
-        const float ox = (float)((gx - 1) * G - Ox), oz = (float)((gz - 1) * G - Oz);
+        const int gx = min(c0[0] + nx, gs0 - 1), gz = min(c0[2] + c, gs2 - 1);
+        const float ox = (float)((gx - 1) * G - ox0), oz = (float)((gz - 1) * G - oz0);
+        const float4 *np = J.nodes + ((uint32_t)gz * (uint32_t)gs1 * (uint32_t)gs0 + (uint32_t)gx);
         float4 v[4];
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const int64_t gy = min(c0[1] + cyb + b, J.gsz[1] - 1);
-            const float4 d = J.nodes[(gz * J.gsz[1] + gy) * J.gsz[0] + gx];
-            v[b] = make_float4(d.x + ox, d.y + (float)((gy - 1) * G - Oy), d.z + oz, 0.f);
+            const int gy = min(c0[1] + cyb + b, gs1 - 1);
+            const float4 d = np[(uint32_t)gy * (uint32_t)gs0];
+            v[b] = make_float4(d.x + ox, d.y + (float)((gy - 1) * G - oy0), d.z + oz, 0.f);
         }
         const float rx = fmaf(wy.x, v[0].x, fmaf(wy.y, v[1].x, fmaf(wy.z, v[2].x, wy.w * v[3].x)));
         const float ry = fmaf(wy.x, v[0].y, fmaf(wy.y, v[1].y, fmaf(wy.z, v[2].y, wy.w * v[3].y)));
