@@ -855,15 +855,32 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     return P;
 }
 
+// Ring barriers come in plane pairs: planes 2p and 2p + 1 (sequence numbers)
+// share the "full" and "empty" mbarriers of pair slot p & (kPairs - 1), so a
+// row warp waits and releases once per two planes.
+constexpr int kPairs = kRing / 2;
+
+__device__ __forceinline__ uint32_t full_bar(const TSmem &S, uint32_t pair)
+{
+    return S.sfull + 8u * (pair & (uint32_t)(kPairs - 1));
+}
+
+__device__ __forceinline__ uint32_t empty_bar(const TSmem &S, uint32_t pair)
+{
+    return S.sfull + 8u * (kRing + (pair & (uint32_t)(kPairs - 1)));
+}
+
 // The producer (lane 0 of the producer warp): copies every source plane of
 // the CTA's staged walks, in walk order, into the ring; plane sequence s
-// goes to slot s & (kRing - 1).  Before it reuses a slot it waits for the
-// slot's "empty" phase: every row warp's reads of the slot's previous plane
-// happen before its arrival there (a release), which the wait observes (an
-// acquire) before the asynchronous write.  seq returns the number of planes
-// issued; false if a wait gave up (or another warp did).
+// goes to slot s & (kRing - 1) and completes on the "full" barrier of its
+// pair s / 2 (two arrivals per phase, one per plane, with the planes'
+// bytes).  Before it reuses a pair slot it waits for the slot's "empty"
+// phase: every row warp's reads of the two planes before happen before its
+// arrival there (a release), which the wait observes (an acquire) before the
+// asynchronous writes.  seq returns the number of planes issued; false if a
+// wait gave up (or another warp did).
 template <typename T, int G>
-__device__ bool produce(const RJob *__restrict__ jobs, int njobs, int64_t total, const Plan *__restrict__ plans,
+__device__ bool produce(const RJob *__restrict__ jobs, int64_t total, const Plan *__restrict__ plans,
                         const TSmem &S, uint32_t &seq)
 {
     using Gm = TGeom<T, G>;
@@ -879,9 +896,10 @@ __device__ bool produce(const RJob *__restrict__ jobs, int njobs, int64_t total,
         }
         const int pfirst = (int)((int64_t)P.z0 + P.a - J.src_o[2]);
         for (int i = 0; i < P.nplanes; ++i, ++seq) {
-            const uint32_t slot = seq & (uint32_t)(kRing - 1);
-            const uint32_t full = S.sfull + 8u * slot, empty = full + 8u * kRing;
-            if (seq >= (uint32_t)kRing && !mbar_wait_producer(empty, (seq / kRing - 1u) & 1u, S.abort))
+            const uint32_t slot = seq & (uint32_t)(kRing - 1), pair = seq >> 1;
+            const uint32_t full = full_bar(S, pair);
+            if ((seq & 1u) == 0 && pair >= (uint32_t)kPairs &&
+                !mbar_wait_producer(empty_bar(S, pair), ((pair / kPairs) - 1u) & 1u, S.abort))
                 return false;
             mbar_expect_tx(full, (uint32_t)(slot == 0 ? 2 : 1) * (uint32_t)Gm::PLANE_B);
             const uint32_t d = S.sring + slot * (uint32_t)Gm::PLANE_B;
@@ -892,41 +910,48 @@ __device__ bool produce(const RJob *__restrict__ jobs, int njobs, int64_t total,
     return true;
 }
 
-// The producer on its way out: every copy it issued has landed before the
-// CTA exits (the row warps waited for all of them unless a wait gave up;
-// bounded waits).
+// The producer on its way out.  An odd number of planes leaves the last
+// pair's barrier one arrival short: it gets a plain arrival, so the phase
+// completes once the copy lands.  Then every copy issued has landed before
+// the CTA exits (the row warps waited for all of them unless a wait gave
+// up; bounded waits).
 __device__ void drain_copies(const TSmem &S, uint32_t seq)
 {
-    const uint32_t n0 = seq > (uint32_t)kRing ? seq - kRing : 0u;
-    for (uint32_t n = n0; n < seq; ++n)
-        if (!mbar_try(S.sfull + 8u * (n % kRing), (n / kRing) & 1u))
-            mbar_wait_slow(S.sfull + 8u * (n % kRing), (n / kRing) & 1u, S.abort, true);
+    if (seq & 1u) mbar_arrive(full_bar(S, seq >> 1));
+    const uint32_t npairs = (seq + 1u) >> 1;
+    const uint32_t n0 = npairs > (uint32_t)kPairs ? npairs - kPairs : 0u;
+    for (uint32_t n = n0; n < npairs; ++n)
+        if (!mbar_try(full_bar(S, n), (n / kPairs) & 1u))
+            mbar_wait_slow(full_bar(S, n), (n / kPairs) & 1u, S.abort, true);
 }
 
-// A row warp's place in the ring: the next plane sequence to wait for and
-// the next to release.  A walk's planes are consecutive sequences, so at
-// the start of a walk rseq = wseq = the sequence of its first plane.
+// A row warp's place in the ring: the next plane pair to wait for and the
+// next plane sequence to release.  A walk's planes are consecutive
+// sequences, so at the start of a walk rseq = the sequence of its first
+// plane.
 struct RingPos {
-    uint32_t wseq, rseq;
+    uint32_t wpair, rseq;
 };
 
-// Waits (bounded) for the planes before sequence `need`; false if a wait
-// gave up.  Every lane waits; the outcome is made uniform across the warp.
+// Waits (bounded) for the planes before sequence `need` (their pairs);
+// false if a wait gave up.  Every lane waits; the outcome is made uniform
+// across the warp.
 __device__ __forceinline__ bool wait_planes(const TSmem &S, RingPos &R, uint32_t need)
 {
-    for (; R.wseq < need; ++R.wseq) {
-        const bool ok = mbar_wait(S.sfull + 8u * (R.wseq & (uint32_t)(kRing - 1)), (R.wseq / kRing) & 1u, S.abort);
+    const uint32_t last = (need - 1u) >> 1;  // the pair of plane need - 1
+    for (; R.wpair <= last; ++R.wpair) {
+        const bool ok = mbar_wait(full_bar(S, R.wpair), (R.wpair / kPairs) & 1u, S.abort);
         if (!__all_sync(0xffffffffu, ok)) return false;
     }
     return true;
 }
 
-// Releases the oldest plane the warp holds: every lane arrives on the slot's
-// "empty" barrier (32 arrivals per row warp), each arrival a release of that
-// lane's reads of the plane.
+// Releases the oldest plane the warp holds.  When it is the second plane of
+// its pair, every lane arrives on the pair's "empty" barrier (32 arrivals
+// per row warp), each arrival a release of that lane's reads of both planes.
 __device__ __forceinline__ void release_plane(const TSmem &S, RingPos &R)
 {
-    mbar_arrive(S.sfull + 8u * (kRing + (R.rseq & (uint32_t)(kRing - 1))));
+    if (R.rseq & 1u) mbar_arrive(empty_bar(S, R.rseq >> 1));
     ++R.rseq;
 }
 
@@ -1082,12 +1107,13 @@ __device__ __forceinline__ uint32_t layer_cz(uint32_t seq0, int64_t Oz, int64_t 
 // same floors, fractions, taps and trilinear arithmetic as pair_staged.
 struct PairPrep {
     float2 fx, fy, fz;
-    const unsigned char *p0, *p1;  // floor taps of voxel 0 / 1 in the ring
+    uint32_t a0, a1;  // shared-window addresses of the floor taps of voxel 0 / 1 in the ring
 };
 
+// ring: shared-window address of slot 0.
 template <typename T>
-__device__ __forceinline__ PairPrep prep_pair(const unsigned char *sm, uint32_t kxy, uint32_t omax, uint32_t cz,
-                                              float2 px, float2 py, float2 pz)
+__device__ __forceinline__ PairPrep prep_pair(uint32_t ring, uint32_t kxy, uint32_t omax, uint32_t cz, float2 px,
+                                              float2 py, float2 pz)
 {
     const float2 MM = f2(kMagic, kMagic);
     const float2 mx = __fadd2_rd(px, MM), my = __fadd2_rd(py, MM), mz = __fadd2_rd(pz, MM);
@@ -1095,23 +1121,37 @@ __device__ __forceinline__ PairPrep prep_pair(const unsigned char *sm, uint32_t 
     q.fx = sub2(px, sub2(mx, MM));
     q.fy = sub2(py, sub2(my, MM));
     q.fz = sub2(pz, sub2(mz, MM));
-    q.p0 = sm + staged_off<T>(kxy, omax, cz, mx.x, my.x, mz.x);
-    q.p1 = sm + staged_off<T>(kxy, omax, cz, mx.y, my.y, mz.y);
+    q.a0 = ring + staged_off<T>(kxy, omax, cz, mx.x, my.x, mz.x);
+    q.a1 = ring + staged_off<T>(kxy, omax, cz, mx.y, my.y, mz.y);
     return q;
 }
 
-// The eight taps of both voxels as magic floats (2^23 + v): constant row,
-// plane and element offsets from each voxel's floor tap.
+// Magic float 2^23 + v of the staged voxel at shared-window address a + OFF:
+// a 32-bit address with the constant offset folded into the load.  Volatile,
+// so it stays after the wait for its plane.
+template <typename T, int OFF>
+__device__ __forceinline__ float lds_mag(uint32_t a)
+{
+    uint32_t v;
+    if (sizeof(T) == 2) asm volatile("ld.shared.u16 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(OFF));
+    else asm volatile("ld.shared.u8 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(OFF));
+    return __int_as_float(0x4B000000 | (int)v);
+}
+
+// The eight taps of both voxels as magic floats: constant row, plane and
+// element offsets from each voxel's floor tap.
 template <typename T>
 __device__ __forceinline__ void taps_pair(const PairPrep &q, float2 (&lo)[4], float2 (&hi)[4])
 {
     constexpr int ES = sizeof(T), ROW_B = kBoxW * ES, PLANE_B = kHMax * ROW_B;
-    constexpr int rofs[4] = {0, ROW_B, PLANE_B, PLANE_B + ROW_B};
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        lo[r] = f2(smag<T>(q.p0 + rofs[r], 0), smag<T>(q.p1 + rofs[r], 0));
-        hi[r] = f2(smag<T>(q.p0 + rofs[r] + ES, 0), smag<T>(q.p1 + rofs[r] + ES, 0));
-    }
+    lo[0] = f2(lds_mag<T, 0>(q.a0), lds_mag<T, 0>(q.a1));
+    hi[0] = f2(lds_mag<T, ES>(q.a0), lds_mag<T, ES>(q.a1));
+    lo[1] = f2(lds_mag<T, ROW_B>(q.a0), lds_mag<T, ROW_B>(q.a1));
+    hi[1] = f2(lds_mag<T, ROW_B + ES>(q.a0), lds_mag<T, ROW_B + ES>(q.a1));
+    lo[2] = f2(lds_mag<T, PLANE_B>(q.a0), lds_mag<T, PLANE_B>(q.a1));
+    hi[2] = f2(lds_mag<T, PLANE_B + ES>(q.a0), lds_mag<T, PLANE_B + ES>(q.a1));
+    lo[3] = f2(lds_mag<T, PLANE_B + ROW_B>(q.a0), lds_mag<T, PLANE_B + ROW_B>(q.a1));
+    hi[3] = f2(lds_mag<T, PLANE_B + ROW_B + ES>(q.a0), lds_mag<T, PLANE_B + ROW_B + ES>(q.a1));
 }
 
 template <typename T>
@@ -1333,7 +1373,7 @@ __device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const
             for (int k = 0; k < NR; ++k) {
                 float2 px, py, pz;
                 pair_positions(wz, PX[k], PY[k], PZ[k], px, py, pz);
-                q[k] = prep_pair<T>(S.base, kxy, omax, cz, px, py, pz);
+                q[k] = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pz);
             }
         };
         PairPrep q[NR];
@@ -1658,9 +1698,9 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
         S.W2[2 * tid] = make_float4(w.x, w.x, w.y, w.y);
         S.W2[2 * tid + 1] = make_float4(w.z, w.z, w.w, w.w);
     }
-    if (tid < kRing) {
-        mbar_init(S.sfull + 8u * tid, 1);
-        mbar_init(S.sfull + 8u * (kRing + tid), 32 * kRowWarps);  // every lane of every row warp
+    if (tid < kPairs) {
+        mbar_init(full_bar(S, tid), 2);                       // one arrival per plane of the pair
+        mbar_init(empty_bar(S, tid), 32 * kRowWarps);         // every lane of every row warp
     }
     if (tid == 0) {
         abort_sh = 0;
@@ -1671,7 +1711,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
     if (warp == kRowWarps) {  // the producer warp: lane 0 issues every copy
         if (lane == 0) {
             uint32_t seq = 0;
-            if (!produce<T, G>(jobs, njobs, total_units, plans, S, seq)) {
+            if (!produce<T, G>(jobs, total_units, plans, S, seq)) {
                 *reinterpret_cast<volatile int *>(&abort_sh) = 1;  // the row warps see it in their waits
                 if (err) atomicOr(err, kKernErrTimeout);
             }
