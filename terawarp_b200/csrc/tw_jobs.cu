@@ -117,7 +117,7 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
         TW_CUDA_TRY(cudaMemsetAsync(fb.p, 0, sizeof(int64_t), st));
     }
     void *d_fb = fb.p;
-    const uint64_t launches = staged ? 3 : 1;
+    const uint64_t launches = staged ? 4 : 1;  // plan, staged (interior walks), staged (other walks), gather
     const size_t bytes = sizeof(RJob) * (size_t)njobs;
     if (njobs <= tw_ctx::kJobsPerSlot && ctx->job_d) {
         // descriptors through the context's slot ring: an asynchronous copy

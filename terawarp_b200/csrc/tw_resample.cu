@@ -855,6 +855,16 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     return P;
 }
 
+// The staged kernel runs in two launches: MODE 0 takes the interior walks
+// (no range tests; its loop stays within the registers of a 17-warp CTA),
+// MODE 1 the other staged walks (the reference's range rule voxel by
+// voxel), so the border code's register needs never reach the interior loop.
+template <int MODE>
+__device__ __forceinline__ bool staged_in_mode(const Plan &P)
+{
+    return P.staged && (MODE == 0 ? P.interior != 0 : P.interior == 0);
+}
+
 // Ring barriers come in plane pairs: planes 2p and 2p + 1 (sequence numbers)
 // share the "full" and "empty" mbarriers of pair slot p & (kPairs - 1), so a
 // row warp waits and releases once per two planes.
@@ -879,7 +889,7 @@ __device__ __forceinline__ uint32_t empty_bar(const TSmem &S, uint32_t pair)
 // arrival there (a release), which the wait observes (an acquire) before the
 // asynchronous writes.  seq returns the number of planes issued; false if a
 // wait gave up (or another warp did).
-template <typename T, int G>
+template <typename T, int G, int MODE>
 __device__ bool produce(const RJob *__restrict__ jobs, int64_t total, const Plan *__restrict__ plans,
                         const TSmem &S, uint32_t &seq)
 {
@@ -888,7 +898,7 @@ __device__ bool produce(const RJob *__restrict__ jobs, int64_t total, const Plan
     int last_job = -1;
     for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
         const Plan P = plans[u];
-        if (!P.staged) continue;
+        if (!staged_in_mode<MODE>(P)) continue;
         const RJob &J = jobs[P.j];
         if (P.j != last_job) {  // the descriptor was written by a copy
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
@@ -1671,7 +1681,7 @@ __global__ void __launch_bounds__(256) k_tps_plan(const RJob *__restrict__ jobs,
 
 // TPS units whose source footprint is staged by TMA (trilinear), with the
 // plans of k_tps_plan; units without a staged plan are left to k_tps_gather.
-template <typename T, int G>
+template <typename T, int G, int MODE>
 __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__restrict__ jobs, int njobs,
                                                                    int64_t total_units, const Plan *__restrict__ plans,
                                                                    int *err)
@@ -1711,7 +1721,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
     if (warp == kRowWarps) {  // the producer warp: lane 0 issues every copy
         if (lane == 0) {
             uint32_t seq = 0;
-            if (!produce<T, G>(jobs, total_units, plans, S, seq)) {
+            if (!produce<T, G, MODE>(jobs, total_units, plans, S, seq)) {
                 *reinterpret_cast<volatile int *>(&abort_sh) = 1;  // the row warps see it in their waits
                 if (err) atomicOr(err, kKernErrTimeout);
             }
@@ -1725,7 +1735,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
     RingPos R = {0u, 0u};
     for (int64_t u = blockIdx.x; u < total_units; u += gridDim.x) {
         const Plan P = plans[u];
-        if (!P.staged) continue;  // the gather kernel takes it
+        if (!staged_in_mode<MODE>(P)) continue;  // the other launch, or the gather kernel, takes it
         Walk w;
         w.j = P.j;
         w.Ox = P.ox;
@@ -1733,8 +1743,9 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
         w.z0 = P.z0;
         w.z1 = P.z1;
         const RJob &J = jobs[w.j];
-        const bool ok = P.interior ? walk_interior<T, G>(J, w, P, S, Rw, wx, R)
-                                   : walk_checked<T, G>(J, w, P, S, Rw, wx, R);
+        bool ok;
+        if constexpr (MODE == 0) ok = walk_interior<T, G>(J, w, P, S, Rw, wx, R);
+        else ok = walk_checked<T, G>(J, w, P, S, Rw, wx, R);
         if (!ok) {
             // the other warps see the flag in their waits and return
             *reinterpret_cast<volatile int *>(&abort_sh) = 1;
@@ -1798,19 +1809,20 @@ cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_
         k_tps_plan<T, G><<<(unsigned)pgrid, 256, 0, st>>>(jobs, njobs, total, plans, fb);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        auto k = k_tps_staged<T, G>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
-        if (e != cudaSuccess) return e;
-        int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kStagedThreads, Gm::smem_bytes);
-        if (e != cudaSuccess) return e;
-        if (per_sm < 1) return cudaErrorInvalidConfiguration;
-        int64_t grid = (int64_t)sms * per_sm;
-        if (grid > total) grid = total;
-        if (grid < 1) grid = 1;
-        k<<<(unsigned)grid, kStagedThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, plans, err);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+        for (auto k : {k_tps_staged<T, G, 0>, k_tps_staged<T, G, 1>}) {  // interior walks, then the others
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
+            if (e != cudaSuccess) return e;
+            int per_sm = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kStagedThreads, Gm::smem_bytes);
+            if (e != cudaSuccess) return e;
+            if (per_sm < 1) return cudaErrorInvalidConfiguration;
+            int64_t grid = (int64_t)sms * per_sm;
+            if (grid > total) grid = total;
+            if (grid < 1) grid = 1;
+            k<<<(unsigned)grid, kStagedThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, plans, err);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
     }
     auto kg = k_tps_gather<T, G, INTERP>;
     int per_sm = 0;
