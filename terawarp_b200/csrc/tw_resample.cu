@@ -821,6 +821,8 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     const int64_t lim = (int64_t)1 << 30;  // TMA coordinates and the plan's coordinates are int32
     if (rx0 < -lim || rx0 > lim || ry0 < -lim || ry0 + rows > lim || p0 < -lim || p1 > lim) return P;
     if (w.Ox > lim || w.Oy > lim || w.z1 > lim) return P;
+    // staged walks index the node grid with 32 bits
+    if (J.gsz[0] * J.gsz[1] * J.gsz[2] >= ((int64_t)1 << 31)) return P;
     P.staged = 1;
     P.a = a;
     P.b = b;
@@ -843,7 +845,6 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     const int64_t ps[3] = {w.Ox, w.Oy, w.z0};
     bool in = w.Ox + kTBX <= J.out_o[0] + J.out_n[0] && w.Oy + kTBY <= J.out_o[1] + J.out_n[1];
     in = in && ((uintptr_t)J.dst) % (2 * sizeof(T)) == 0 && J.dst_py % 2 == 0 && J.dst_pz % 2 == 0;
-    in = in && J.gsz[0] * J.gsz[1] * J.gsz[2] < ((int64_t)1 << 31);  // node indices of interior walks are 32-bit
     for (int ax = 0; ax < 3; ++ax) {
         const double lo = (double)ps[ax] + (double)mn[ax] - (double)e;
         const double hi = (double)pe[ax] + (double)mx[ax] + (double)e;
@@ -1171,11 +1172,11 @@ __device__ __forceinline__ uint32_t finish_pair(const PairPrep &q, const float2 
     return pack_pair<T>(__float_as_uint(t.x), __float_as_uint(t.y));
 }
 
-// Cell-layer set-up of row warp y of an interior walk: the y contraction of
+// Cell-layer set-up of row warp y of a staged walk: the y contraction of
 // the row's nodes into Rw, then the lane's x contraction into position pairs
 // per node layer c: PX[c] = (x of voxel 0, x of voxel 1), PY[c], PZ[c]
-// likewise.  Same operations and order as row_layer (the other walks), so a
-// voxel's position does not depend on which path sampled it.
+// likewise.  Same operations and order as row_layer (the gather kernel), so
+// a voxel's position does not depend on which path sampled it.
 template <typename T, int G>
 __device__ __forceinline__ void layer_positions(const RJob &J, int64_t Ox, int64_t Oy, int64_t Oz, int y,
                                                 const float4 *W, float4 *Rw, const float4 (&wx)[2], float2 (&PX)[4],
@@ -1183,8 +1184,9 @@ __device__ __forceinline__ void layer_positions(const RJob &J, int64_t Ox, int64
 {
     using Gm = TGeom<T, G>;
     const int lane = threadIdx.x & 31;
-    // interior walks have int32 coordinates and node indices (the planning
-    // kernel checks the coordinates; node grids stay below 2^31 nodes)
+    // staged walks have int32 coordinates and node indices (the planning
+    // kernel stages a walk only when its coordinates are below 2^30 and the
+    // node grid below 2^31 nodes)
     const int ox0 = (int)Ox, oy0 = (int)Oy, oz0 = (int)Oz;
     const int c0[3] = {ox0 / G, oy0 / G, oz0 / G};
     const int gs0 = (int)J.gsz[0], gs1 = (int)J.gsz[1], gs2 = (int)J.gsz[2];
@@ -1413,67 +1415,73 @@ __device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const
     return true;
 }
 
-// Row warp y's part of any other staged walk (rows y and y + kRowWarps):
-// the layer's sample hull decides per row and plane between the unchecked
-// staged sample and the checked one (the reference's range rule per voxel,
-// taps clamped into the staged window).  false if a wait gave up.
+// Row warp y's part of any other staged walk (one that reaches the volume's
+// or the source buffer's faces, or a partial unit).  The same node
+// contractions and positions as an interior walk; per output plane the warp
+// votes: when every lane's voxel pair is whole, storable as one word, and
+// safely inside (floor(q) >= the lowest valid index and floor(q) + 1 <= the
+// highest, in every axis, for both voxels), the plane takes the interior
+// sample; otherwise the reference's range rule is applied voxel by voxel,
+// taps clamped into the staged window.  A valid sample gives the same bits
+// on either path.  false if a wait gave up.
 template <typename T, int G>
 __device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
                              const float4 (&wx)[2], RingPos &R)
 {
     using Gm = TGeom<T, G>;
-    const int lane = threadIdx.x & 31;
+    const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int x = 2 * lane;
     const uint32_t seq0 = R.rseq;
     const uint32_t Wn = (uint32_t)(P.b - P.a + 1);
     const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
+    const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;  // uniform across the warp
     const int64_t dst_pz = J.dst_pz;
     // a voxel pair (even x) can be written as one 2-element store
     const bool pair_ok = (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
+    const bool lane_whole = pair_ok && x + 2 <= xe;
     const uint32_t kxy =
         (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
     const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
-    const int y0 = threadIdx.x >> 5;
     T *drow = static_cast<T *>(J.dst) +
-              ((w.z0 - J.out_o[2]) * dst_pz + (w.Oy + y0 - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
-    const int64_t drow2 = kRowWarps * J.dst_py;
+              ((w.z0 - J.out_o[2]) * dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
     for (int64_t zf = w.z0; zf < w.z1;) {
         const int64_t ze = min(w.z1, (zf / G + 1) * G);
         const int64_t Oz = (zf / G) * G;
-        const int zoff = (int)(zf - Oz), zn = (int)(ze - zf);
-        RowLayer L[kRowsPerWarp];
-        bool rowv[kRowsPerWarp];
-#pragma unroll
-        for (int k = 0; k < kRowsPerWarp; ++k) {
-            const int y = y0 + k * kRowWarps;
-            rowv[k] = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;
-            if (rowv[k]) row_layer<T, G>(J, w.Ox, w.Oy, Oz, zoff, zn, y, xe, S.W, Rw, wx, L[k]);
-        }
+        const int zoff = (int)(zf - Oz), zend = (int)(ze - Oz);
+        float2 PX[4], PY[4], PZ[4];
+        if (rowv) layer_positions<T, G>(J, w.Ox, w.Oy, Oz, y, S.W, Rw, wx, PX, PY, PZ);
+        const int64_t O[3] = {w.Ox, w.Oy, Oz};
+        const Frame fr = make_frame(J, O);
+        // q in [lb, hb) per axis: both taps inside the volume and the buffer
+        const float lbx = fmaxf(fr.lo[0], (float)fr.bl[0]), hbx = fminf(fr.hi[0], (float)fr.bh[0]);
+        const float lby = fmaxf(fr.lo[1], (float)fr.bl[1]), hby = fminf(fr.hi[1], (float)fr.bh[1]);
+        const float lbz = fmaxf(fr.lo[2], (float)fr.bl[2]), hbz = fminf(fr.hi[2], (float)fr.bh[2]);
         const uint32_t cz = layer_cz(seq0, Oz, w.z0, P.a);
         uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
-        for (int pz = zoff; pz < zoff + zn; ++pz, ++need) {  // frame z of the plane
+        for (int pz = zoff; pz < zend; ++pz, ++need) {  // frame z of the plane
             if (!wait_planes(S, R, need)) return false;
-#pragma unroll
-            for (int k = 0; k < kRowsPerWarp; ++k) {
-                if (!rowv[k]) continue;
-                T *dr = drow + k * drow2;
-                float2 p0, p1, pz2;
-                plane_positions(L[k], S.W[pz], p0, p1, pz2);
-                const float fz = (float)pz;
-                if (L[k].row_fast && fz >= L[k].zlo && fz < L[k].zhi) {
-                    const Frame unused = {};
-                    const float wl[3] = {0.f, 0.f, 0.f}, wh[3] = {0.f, 0.f, 0.f};
-                    const uint32_t v = pair_staged<T, false>(S.base, kxy, omax, cz, p0, p1, pz2, unused, wl, wh, 2);
-                    store_packed<T>(dr + x, v, pair_ok, 2);
+            if (rowv) {
+                const float4 wa = S.W2[2 * pz], wb = S.W2[2 * pz + 1];
+                const float2 wz[4] = {f2(wa.x, wa.y), f2(wa.z, wa.w), f2(wb.x, wb.y), f2(wb.z, wb.w)};
+                float2 px, py, pzz;
+                pair_positions(wz, PX, PY, PZ, px, py, pzz);
+                const bool safe = lane_whole && fminf(px.x, px.y) >= lbx && fmaxf(px.x, px.y) < hbx &&
+                                  fminf(py.x, py.y) >= lby && fmaxf(py.x, py.y) < hby &&
+                                  fminf(pzz.x, pzz.y) >= lbz && fmaxf(pzz.x, pzz.y) < hbz;
+                if (__all_sync(0xffffffffu, safe)) {
+                    const PairPrep q = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pzz);
+                    float2 lo[4], hi[4];
+                    taps_pair<T>(q, lo, hi);
+                    const uint32_t v = finish_pair<T>(q, lo, hi);
+                    if (sizeof(T) == 2) *reinterpret_cast<uint32_t *>(drow + x) = v;
+                    else *reinterpret_cast<uint16_t *>(drow + x) = (uint16_t)v;
                 } else if (x < xe) {
-                    const int64_t O[3] = {w.Ox, w.Oy, Oz};
-                    const Frame frame = make_frame(J, O);
                     const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(pz + P.a)};
                     const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
                                          (float)(pz + P.b - 1)};
-                    const uint32_t v =
-                        pair_staged<T, true>(S.base, kxy, omax, cz, p0, p1, pz2, frame, wl, wh, xe - x);
-                    store_packed<T>(dr + x, v, pair_ok, xe - x);
+                    const uint32_t v = pair_staged<T, true>(S.base, kxy, omax, cz, f2(px.x, py.x), f2(px.y, py.y),
+                                                            pzz, fr, wl, wh, xe - x);
+                    store_packed<T>(drow + x, v, pair_ok, xe - x);
                 }
             }
             drow += dst_pz;
