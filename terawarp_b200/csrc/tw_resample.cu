@@ -1080,13 +1080,6 @@ __device__ __forceinline__ void plane_positions(const RowLayer &L, float4 wz, fl
     pz = fma2(w0, L.P[0][2], fma2(w1, L.P[1][2], fma2(w2, L.P[2][2], fma2(w3, L.P[3][2], f2(0.f, 0.f)))));
 }
 
-// Magic float 2^23 + v of the staged voxel at offset o.
-template <typename T>
-__device__ __forceinline__ float smag(const unsigned char *sm, uint32_t o)
-{
-    return __int_as_float(0x4B000000 | (int)(uint32_t)*reinterpret_cast<const T *>(sm + o));
-}
-
 // Offset (from the ring base) of the (x, y, z) = floor tap of a staged
 // sample, from the magic-floor bit patterns; cz maps a tap plane to its
 // plane sequence (mod kRing: the slot); clamped so that all 8 taps stay in
@@ -1115,7 +1108,8 @@ __device__ __forceinline__ uint32_t layer_cz(uint32_t seq0, int64_t Oz, int64_t 
 // and the two floor taps' addresses (prep), the eight taps of both voxels
 // are loaded (taps), and the trilinear value is rounded and packed
 // (finish).  No range tests: every tap is inside the staged window.  The
-// same floors, fractions, taps and trilinear arithmetic as pair_staged.
+// same floors, fractions and trilinear arithmetic (trilerp2) as the gather
+// kernel's samplers.
 struct PairPrep {
     float2 fx, fy, fz;
     uint32_t a0, a1;  // shared-window addresses of the floor taps of voxel 0 / 1 in the ring
@@ -1234,59 +1228,6 @@ __device__ __forceinline__ void layer_positions(const RJob &J, int64_t Ox, int64
     }
 }
 
-
-// A voxel pair sampled from the staged planes.  CHECKED applies the
-// reference's range rule per voxel (0 <= q <= sz-1, else 0) and clamps floor(q)
-// into the staged window (wl, wh: frame coordinates) so that no tap of an
-// invalid sample leaves it; for a valid sample the clamp changes nothing (the
-// window holds the whole footprint), so both variants give the same bits.
-template <typename T, bool CHECKED>
-__device__ __forceinline__ uint32_t pair_staged(const unsigned char *sm, uint32_t kxy, uint32_t omax, uint32_t cz,
-                                                float2 p0, float2 p1, float2 pz2, const Frame &f, const float (&wl)[3],
-                                                const float (&wh)[3], int nvalid)
-{
-    constexpr uint32_t ES = sizeof(T), ROW_B = kBoxW * ES, PLANE_B = kHMax * ROW_B;
-    const float2 MM = f2(kMagic, kMagic);
-    float2 m0, m1, mz, f0, f1, fz;
-    bool ok0 = true, ok1 = true;
-    if (CHECKED) {
-        ok0 = nvalid >= 1 && p0.x >= f.lo[0] && p0.x <= f.hi[0] && p0.y >= f.lo[1] && p0.y <= f.hi[1] &&
-              pz2.x >= f.lo[2] && pz2.x <= f.hi[2];
-        ok1 = nvalid >= 2 && p1.x >= f.lo[0] && p1.x <= f.hi[0] && p1.y >= f.lo[1] && p1.y <= f.hi[1] &&
-              pz2.y >= f.lo[2] && pz2.y <= f.hi[2];
-        float2 l0 = sub2(__fadd2_rd(p0, MM), MM), l1 = sub2(__fadd2_rd(p1, MM), MM);
-        float2 lz2 = sub2(__fadd2_rd(pz2, MM), MM);
-        l0 = f2(fminf(fmaxf(l0.x, wl[0]), wh[0]), fminf(fmaxf(l0.y, wl[1]), wh[1]));
-        l1 = f2(fminf(fmaxf(l1.x, wl[0]), wh[0]), fminf(fmaxf(l1.y, wl[1]), wh[1]));
-        lz2 = f2(fminf(fmaxf(lz2.x, wl[2]), wh[2]), fminf(fmaxf(lz2.y, wl[2]), wh[2]));
-        f0 = sub2(p0, l0);
-        f1 = sub2(p1, l1);
-        fz = sub2(pz2, lz2);
-        m0 = add2(l0, MM);  // exact: integers
-        m1 = add2(l1, MM);
-        mz = add2(lz2, MM);
-    } else {
-        m0 = __fadd2_rd(p0, MM);
-        m1 = __fadd2_rd(p1, MM);
-        mz = __fadd2_rd(pz2, MM);
-        f0 = sub2(p0, sub2(m0, MM));
-        f1 = sub2(p1, sub2(m1, MM));
-        fz = sub2(pz2, sub2(mz, MM));
-    }
-    const uint32_t o0 = staged_off<T>(kxy, omax, cz, m0.x, m0.y, mz.x);
-    const uint32_t o1 = staged_off<T>(kxy, omax, cz, m1.x, m1.y, mz.y);
-    constexpr uint32_t rofs[4] = {0u, ROW_B, PLANE_B, PLANE_B + ROW_B};
-    float2 lo[4], hi[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {  // constant offsets from the floor taps' addresses
-        lo[r] = f2(smag<T>(sm + o0 + rofs[r], 0), smag<T>(sm + o1 + rofs[r], 0));
-        hi[r] = f2(smag<T>(sm + o0 + rofs[r] + ES, 0), smag<T>(sm + o1 + rofs[r] + ES, 0));
-    }
-    const float2 t = out_pair<T, true>(trilerp2(lo, hi, f2(f0.x, f1.x), f2(f0.y, f1.y), fz));
-    if (CHECKED)  // a rejected voxel writes 0: the bits of 2^23 have zero low bits
-        return pack_pair<T>(ok0 ? __float_as_uint(t.x) : 0x4B000000u, ok1 ? __float_as_uint(t.y) : 0x4B000000u);
-    return pack_pair<T>(__float_as_uint(t.x), __float_as_uint(t.y));
-}
 
 // Global-memory sampling state of a row warp's layer (every path but the staged one).
 template <typename T>
@@ -1416,14 +1357,19 @@ __device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const
 }
 
 // Row warp y's part of any other staged walk (one that reaches the volume's
-// or the source buffer's faces, or a partial unit).  The same node
-// contractions and positions as an interior walk; per output plane the warp
-// votes: when every lane's voxel pair is whole, storable as one word, and
-// safely inside (floor(q) >= the lowest valid index and floor(q) + 1 <= the
-// highest, in every axis, for both voxels), the plane takes the interior
-// sample; otherwise the reference's range rule is applied voxel by voxel,
-// taps clamped into the staged window.  A valid sample gives the same bits
-// on either path.  false if a wait gave up.
+// or the source buffer's faces, or a partial unit): the interior walk's
+// arithmetic, then the reference's range rule as a mask (a sample with any
+// q outside [0, sz - 1] writes 0) and stores limited to the output region.
+// This gives the checked sample's bits for every voxel:
+//  - the staged window holds the floor tap and the +1 tap of every sample of
+//    the walk, zero-filled where it reaches past the source, and a tap
+//    offset is clamped into the ring whatever the position, so no position
+//    reads outside shared memory;
+//  - a valid sample's taps are inside the volume and the source buffer, but
+//    for q = sz - 1 exactly, whose +1 tap has weight 0 (lo + 0 (hi - lo) =
+//    lo exactly, as the clamped floor sz - 2 with fraction 1 gives hi);
+//  - an invalid sample (NaN included: every comparison fails) is masked.
+// false if a wait gave up.
 template <typename T, int G>
 __device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
                              const float4 (&wx)[2], RingPos &R)
@@ -1435,15 +1381,16 @@ __device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const 
     const uint32_t Wn = (uint32_t)(P.b - P.a + 1);
     const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
     const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;  // uniform across the warp
-    const int64_t dst_pz = J.dst_pz;
     // a voxel pair (even x) can be written as one 2-element store
     const bool pair_ok = (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
-    const bool lane_whole = pair_ok && x + 2 <= xe;
+    constexpr uint32_t M0 = sizeof(T) == 2 ? 0xFFFFu : 0xFFu;
+    constexpr uint32_t M1 = sizeof(T) == 2 ? 0xFFFF0000u : 0xFF00u;
     const uint32_t kxy =
         (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
     const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
-    T *drow = static_cast<T *>(J.dst) +
-              ((w.z0 - J.out_o[2]) * dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0]));
+    const int64_t dpz = J.dst_pz;
+    T *dp = static_cast<T *>(J.dst) +
+            ((w.z0 - J.out_o[2]) * dpz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0])) + x;
     for (int64_t zf = w.z0; zf < w.z1;) {
         const int64_t ze = min(w.z1, (zf / G + 1) * G);
         const int64_t Oz = (zf / G) * G;
@@ -1451,11 +1398,7 @@ __device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const 
         float2 PX[4], PY[4], PZ[4];
         if (rowv) layer_positions<T, G>(J, w.Ox, w.Oy, Oz, y, S.W, Rw, wx, PX, PY, PZ);
         const int64_t O[3] = {w.Ox, w.Oy, Oz};
-        const Frame fr = make_frame(J, O);
-        // q in [lb, hb) per axis: both taps inside the volume and the buffer
-        const float lbx = fmaxf(fr.lo[0], (float)fr.bl[0]), hbx = fminf(fr.hi[0], (float)fr.bh[0]);
-        const float lby = fmaxf(fr.lo[1], (float)fr.bl[1]), hby = fminf(fr.hi[1], (float)fr.bh[1]);
-        const float lbz = fmaxf(fr.lo[2], (float)fr.bl[2]), hbz = fminf(fr.hi[2], (float)fr.bh[2]);
+        const Frame fr = make_frame(J, O);  // valid samples: lo <= q <= hi per axis (frame coordinates)
         const uint32_t cz = layer_cz(seq0, Oz, w.z0, P.a);
         uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
         for (int pz = zoff; pz < zend; ++pz, ++need) {  // frame z of the plane
@@ -1465,26 +1408,17 @@ __device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const 
                 const float2 wz[4] = {f2(wa.x, wa.y), f2(wa.z, wa.w), f2(wb.x, wb.y), f2(wb.z, wb.w)};
                 float2 px, py, pzz;
                 pair_positions(wz, PX, PY, PZ, px, py, pzz);
-                const bool safe = lane_whole && fminf(px.x, px.y) >= lbx && fmaxf(px.x, px.y) < hbx &&
-                                  fminf(py.x, py.y) >= lby && fmaxf(py.x, py.y) < hby &&
-                                  fminf(pzz.x, pzz.y) >= lbz && fmaxf(pzz.x, pzz.y) < hbz;
-                if (__all_sync(0xffffffffu, safe)) {
-                    const PairPrep q = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pzz);
-                    float2 lo[4], hi[4];
-                    taps_pair<T>(q, lo, hi);
-                    const uint32_t v = finish_pair<T>(q, lo, hi);
-                    if (sizeof(T) == 2) *reinterpret_cast<uint32_t *>(drow + x) = v;
-                    else *reinterpret_cast<uint16_t *>(drow + x) = (uint16_t)v;
-                } else if (x < xe) {
-                    const float wl[3] = {(float)(-P.DX), (float)(-P.DY), (float)(pz + P.a)};
-                    const float wh[3] = {(float)(kBoxW - 2 - P.DX), (float)(P.rows - 2 - P.DY),
-                                         (float)(pz + P.b - 1)};
-                    const uint32_t v = pair_staged<T, true>(S.base, kxy, omax, cz, f2(px.x, py.x), f2(px.y, py.y),
-                                                            pzz, fr, wl, wh, xe - x);
-                    store_packed<T>(drow + x, v, pair_ok, xe - x);
-                }
+                const PairPrep q = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pzz);
+                float2 lo[4], hi[4];
+                taps_pair<T>(q, lo, hi);
+                const uint32_t v = finish_pair<T>(q, lo, hi);
+                const bool ok0 = px.x >= fr.lo[0] && px.x <= fr.hi[0] && py.x >= fr.lo[1] && py.x <= fr.hi[1] &&
+                                 pzz.x >= fr.lo[2] && pzz.x <= fr.hi[2];
+                const bool ok1 = px.y >= fr.lo[0] && px.y <= fr.hi[0] && py.y >= fr.lo[1] && py.y <= fr.hi[1] &&
+                                 pzz.y >= fr.lo[2] && pzz.y <= fr.hi[2];
+                if (x < xe) store_packed<T>(dp, v & ((ok0 ? M0 : 0u) | (ok1 ? M1 : 0u)), pair_ok, xe - x);
             }
-            drow += dst_pz;
+            dp += dpz;
             release_plane(S, R);  // the window start is not read by later planes
         }
         zf = ze;
