@@ -1285,23 +1285,52 @@ __device__ __forceinline__ void pair_positions(const float2 (&w)[4], const float
     pz = fma2(w[0], PZ[0], fma2(w[1], PZ[1], fma2(w[2], PZ[2], fma2(w[3], PZ[3], Z2))));
 }
 
-// Row warp y's part of an interior walk (every sample inside: no range
-// tests, whole rows, paired stores): rows y + k kRowWarps (k < kRowsPerWarp),
-// whose voxel pairs are independent work for the lane.  Per output plane z
-// it waits for the planes up to z + b, samples, stores, and releases plane
-// z + a, which no later plane of the walk reads.  false if a wait gave up.
-template <typename T, int G>
-__device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
-                              const float4 (&wx)[2], RingPos &R)
+// Row warp y's part of a staged walk: rows y + k kRowWarps (k <
+// kRowsPerWarp), whose voxel pairs are independent work for the lane.  Per
+// output plane z it waits for the planes up to z + b, samples, stores, and
+// releases plane z + a, which no later plane of the walk reads; the
+// fractions and tap addresses of a plane are computed during the plane
+// before it (they need no staged data), so that their arithmetic overlaps
+// the previous plane's loads.
+//
+// An interior walk (BORDER false: every sample inside, whole rows, paired
+// stores) runs no range test.  Any other staged walk (one that reaches the
+// volume's or the source buffer's faces, or a partial unit) runs the same
+// arithmetic, then the reference's range rule as a mask (a sample with any
+// q outside [0, sz - 1] writes 0), and stores only inside the output
+// region.  This gives the checked sample's bits for every voxel:
+//  - the staged window holds the floor tap and the +1 tap of every sample of
+//    the walk, zero-filled where it reaches past the source, and a tap
+//    offset is clamped into the ring whatever the position, so no position
+//    reads outside shared memory;
+//  - a valid sample's taps are inside the volume and the source buffer, but
+//    for q = sz - 1 exactly, whose +1 tap has weight 0 (lo + 0 (hi - lo) =
+//    lo exactly, as the clamped floor sz - 2 with fraction 1 gives hi);
+//  - an invalid sample (NaN included: every comparison fails) is masked.
+// false if a wait gave up.
+template <typename T, int G, bool BORDER>
+__device__ bool walk_rows(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
+                          const float4 (&wx)[2], RingPos &R)
 {
     using Gm = TGeom<T, G>;
     constexpr int NR = kRowsPerWarp;
+    constexpr uint32_t M0 = sizeof(T) == 2 ? 0xFFFFu : 0xFFu;
+    constexpr uint32_t M1 = sizeof(T) == 2 ? 0xFFFF0000u : 0xFF00u;
     const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int x = 2 * lane;
     const uint32_t seq0 = R.rseq;   // sequence of the walk's first plane
     const uint32_t Wn = (uint32_t)(P.b - P.a + 1);  // planes of a window
     T *dp = static_cast<T *>(J.dst) +
-            ((w.z0 - J.out_o[2]) * J.dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0])) + 2 * lane;
+            ((w.z0 - J.out_o[2]) * J.dst_pz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0])) + x;
     const int64_t dpz = J.dst_pz, drow2 = kRowWarps * J.dst_py;
+    // border walks: rows inside the output region (uniform across the warp),
+    // the lane's valid voxels, whether a pair can be stored as one word
+    bool rowv[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) rowv[k] = !BORDER || (int64_t)(y + k * kRowWarps) < J.out_o[1] + J.out_n[1] - w.Oy;
+    const int xe = BORDER ? (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX) : kTBX;
+    const bool pair_ok =
+        !BORDER || ((((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0));
     // frame (0, 0) in slot 0 minus the magic-float bias of the floor bit
     // patterns (2^32 wrap arithmetic)
     const uint32_t kxy =
@@ -1314,12 +1343,15 @@ __device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const
         float2 PX[NR][4], PY[NR][4], PZ[NR][4];
 #pragma unroll
         for (int k = 0; k < NR; ++k)
-            layer_positions<T, G>(J, w.Ox, w.Oy, Oz, y + k * kRowWarps, S.W, Rw, wx, PX[k], PY[k], PZ[k]);
+            if (rowv[k])
+                layer_positions<T, G>(J, w.Ox, w.Oy, Oz, y + k * kRowWarps, S.W, Rw, wx, PX[k], PY[k], PZ[k]);
+        Frame fr;  // valid samples: lo <= q <= hi per axis (frame coordinates)
+        if (BORDER) {
+            const int64_t O[3] = {w.Ox, w.Oy, Oz};
+            fr = make_frame(J, O);
+        }
         const uint32_t cz = layer_cz(seq0, Oz, w.z0, P.a);
-        // the fractions and tap addresses of plane pz are computed during
-        // plane pz - 1 (they need no staged data), so that their arithmetic
-        // overlaps the previous plane's loads
-        auto prep = [&](int p, PairPrep (&q)[NR]) {
+        auto prep = [&](int p, PairPrep (&q)[NR], uint32_t (&keep)[NR]) {
             const float4 wa = S.W2[2 * p], wb = S.W2[2 * p + 1];
             const float2 wz[4] = {f2(wa.x, wa.y), f2(wa.z, wa.w), f2(wb.x, wb.y), f2(wb.z, wb.w)};
 #pragma unroll
@@ -1327,10 +1359,18 @@ __device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const
                 float2 px, py, pz;
                 pair_positions(wz, PX[k], PY[k], PZ[k], px, py, pz);
                 q[k] = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pz);
+                if (BORDER) {
+                    const bool ok0 = px.x >= fr.lo[0] && px.x <= fr.hi[0] && py.x >= fr.lo[1] && py.x <= fr.hi[1] &&
+                                     pz.x >= fr.lo[2] && pz.x <= fr.hi[2];
+                    const bool ok1 = px.y >= fr.lo[0] && px.y <= fr.hi[0] && py.y >= fr.lo[1] && py.y <= fr.hi[1] &&
+                                     pz.y >= fr.lo[2] && pz.y <= fr.hi[2];
+                    keep[k] = (ok0 ? M0 : 0u) | (ok1 ? M1 : 0u);
+                }
             }
         };
         PairPrep q[NR];
-        prep(zoff, q);
+        uint32_t keep[NR];
+        prep(zoff, q, keep);
         // sequence past the last plane output plane Oz + pz reads
         uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
         for (int pz = zoff; pz < zend; ++pz, ++need) {
@@ -1339,87 +1379,22 @@ __device__ bool walk_interior(const RJob &J, const Walk &w, const Plan &P, const
 #pragma unroll
             for (int k = 0; k < NR; ++k) taps_pair<T>(q[k], lo[k], hi[k]);
             PairPrep nq[NR];
-            prep(min(pz + 1, G - 1), nq);  // (the last plane's is not used)
+            uint32_t nkeep[NR];
+            prep(min(pz + 1, G - 1), nq, nkeep);  // (the last plane's is not used)
 #pragma unroll
             for (int k = 0; k < NR; ++k) {
                 const uint32_t v = finish_pair<T>(q[k], lo[k], hi[k]);
-                if (sizeof(T) == 2) *reinterpret_cast<uint32_t *>(dp + k * drow2) = v;
-                else *reinterpret_cast<uint16_t *>(dp + k * drow2) = (uint16_t)v;
+                if (!BORDER) {
+                    if (sizeof(T) == 2) *reinterpret_cast<uint32_t *>(dp + k * drow2) = v;
+                    else *reinterpret_cast<uint16_t *>(dp + k * drow2) = (uint16_t)v;
+                } else if (rowv[k] && x < xe) {
+                    store_packed<T>(dp + k * drow2, v & keep[k], pair_ok, xe - x);
+                }
                 q[k] = nq[k];
+                if (BORDER) keep[k] = nkeep[k];
             }
             dp += dpz;
             release_plane(S, R);
-        }
-        zf = ze;
-    }
-    for (uint32_t i = 1; i < Wn; ++i) release_plane(S, R);  // the rest of the last window
-    return true;
-}
-
-// Row warp y's part of any other staged walk (one that reaches the volume's
-// or the source buffer's faces, or a partial unit): the interior walk's
-// arithmetic, then the reference's range rule as a mask (a sample with any
-// q outside [0, sz - 1] writes 0) and stores limited to the output region.
-// This gives the checked sample's bits for every voxel:
-//  - the staged window holds the floor tap and the +1 tap of every sample of
-//    the walk, zero-filled where it reaches past the source, and a tap
-//    offset is clamped into the ring whatever the position, so no position
-//    reads outside shared memory;
-//  - a valid sample's taps are inside the volume and the source buffer, but
-//    for q = sz - 1 exactly, whose +1 tap has weight 0 (lo + 0 (hi - lo) =
-//    lo exactly, as the clamped floor sz - 2 with fraction 1 gives hi);
-//  - an invalid sample (NaN included: every comparison fails) is masked.
-// false if a wait gave up.
-template <typename T, int G>
-__device__ bool walk_checked(const RJob &J, const Walk &w, const Plan &P, const TSmem &S, float4 *Rw,
-                             const float4 (&wx)[2], RingPos &R)
-{
-    using Gm = TGeom<T, G>;
-    const int y = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x = 2 * lane;
-    const uint32_t seq0 = R.rseq;
-    const uint32_t Wn = (uint32_t)(P.b - P.a + 1);
-    const int xe = (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX);
-    const bool rowv = (int64_t)y < J.out_o[1] + J.out_n[1] - w.Oy;  // uniform across the warp
-    // a voxel pair (even x) can be written as one 2-element store
-    const bool pair_ok = (((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0);
-    constexpr uint32_t M0 = sizeof(T) == 2 ? 0xFFFFu : 0xFFu;
-    constexpr uint32_t M1 = sizeof(T) == 2 ? 0xFFFF0000u : 0xFF00u;
-    const uint32_t kxy =
-        (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
-    const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
-    const int64_t dpz = J.dst_pz;
-    T *dp = static_cast<T *>(J.dst) +
-            ((w.z0 - J.out_o[2]) * dpz + (w.Oy + y - J.out_o[1]) * J.dst_py + (w.Ox - J.out_o[0])) + x;
-    for (int64_t zf = w.z0; zf < w.z1;) {
-        const int64_t ze = min(w.z1, (zf / G + 1) * G);
-        const int64_t Oz = (zf / G) * G;
-        const int zoff = (int)(zf - Oz), zend = (int)(ze - Oz);
-        float2 PX[4], PY[4], PZ[4];
-        if (rowv) layer_positions<T, G>(J, w.Ox, w.Oy, Oz, y, S.W, Rw, wx, PX, PY, PZ);
-        const int64_t O[3] = {w.Ox, w.Oy, Oz};
-        const Frame fr = make_frame(J, O);  // valid samples: lo <= q <= hi per axis (frame coordinates)
-        const uint32_t cz = layer_cz(seq0, Oz, w.z0, P.a);
-        uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
-        for (int pz = zoff; pz < zend; ++pz, ++need) {  // frame z of the plane
-            if (!wait_planes(S, R, need)) return false;
-            if (rowv) {
-                const float4 wa = S.W2[2 * pz], wb = S.W2[2 * pz + 1];
-                const float2 wz[4] = {f2(wa.x, wa.y), f2(wa.z, wa.w), f2(wb.x, wb.y), f2(wb.z, wb.w)};
-                float2 px, py, pzz;
-                pair_positions(wz, PX, PY, PZ, px, py, pzz);
-                const PairPrep q = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pzz);
-                float2 lo[4], hi[4];
-                taps_pair<T>(q, lo, hi);
-                const uint32_t v = finish_pair<T>(q, lo, hi);
-                const bool ok0 = px.x >= fr.lo[0] && px.x <= fr.hi[0] && py.x >= fr.lo[1] && py.x <= fr.hi[1] &&
-                                 pzz.x >= fr.lo[2] && pzz.x <= fr.hi[2];
-                const bool ok1 = px.y >= fr.lo[0] && px.y <= fr.hi[0] && py.y >= fr.lo[1] && py.y <= fr.hi[1] &&
-                                 pzz.y >= fr.lo[2] && pzz.y <= fr.hi[2];
-                if (x < xe) store_packed<T>(dp, v & ((ok0 ? M0 : 0u) | (ok1 ? M1 : 0u)), pair_ok, xe - x);
-            }
-            dp += dpz;
-            release_plane(S, R);  // the window start is not read by later planes
         }
         zf = ze;
     }
@@ -1685,9 +1660,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
         w.z0 = P.z0;
         w.z1 = P.z1;
         const RJob &J = jobs[w.j];
-        bool ok;
-        if constexpr (MODE == 0) ok = walk_interior<T, G>(J, w, P, S, Rw, wx, R);
-        else ok = walk_checked<T, G>(J, w, P, S, Rw, wx, R);
+        const bool ok = walk_rows<T, G, MODE == 1>(J, w, P, S, Rw, wx, R);
         if (!ok) {
             // the other warps see the flag in their waits and return
             *reinterpret_cast<volatile int *>(&abort_sh) = 1;
