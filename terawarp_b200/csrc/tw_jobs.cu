@@ -117,7 +117,8 @@ tw_status run_jobs(tw_ctx *ctx, RJob *jobs, int njobs, cudaStream_t st)
         TW_CUDA_TRY(cudaMemsetAsync(fb.p, 0, sizeof(int64_t), st));
     }
     void *d_fb = fb.p;
-    const uint64_t launches = staged ? 4 : 1;  // plan, staged (interior walks), staged (other walks), gather
+    // plan, walk lists, staged (interior walks), staged (other walks), gather
+    const uint64_t launches = staged ? 5 : 1;
     const size_t bytes = sizeof(RJob) * (size_t)njobs;
     if (njobs <= tw_ctx::kJobsPerSlot && ctx->job_d) {
         // descriptors through the context's slot ring: an asynchronous copy

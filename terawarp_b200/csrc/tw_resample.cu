@@ -856,15 +856,15 @@ __device__ Plan plan_walk(const RJob &J, const Walk &w)
     return P;
 }
 
-// The staged kernel runs in two launches: MODE 0 takes the interior walks
-// (no range tests; its loop stays within the registers of a 17-warp CTA),
-// MODE 1 the other staged walks (the reference's range rule voxel by
-// voxel), so the border code's register needs never reach the interior loop.
-template <int MODE>
-__device__ __forceinline__ bool staged_in_mode(const Plan &P)
-{
-    return P.staged && (MODE == 0 ? P.interior != 0 : P.interior == 0);
-}
+// The staged kernel runs in two launches: MODE 0 takes the interior walks,
+// MODE 1 the other staged walks (the reference's range rule as a mask).
+// Each launch strides over its own list of walks, in unit order, which
+// k_tps_lists builds: strided over all units, the CTAs met the border walks
+// unevenly (148 CTAs and 32 columns per row of a 2048-wide job share the
+// factor 4, so half the CTAs took every x-face walk), and the launch waited
+// for the busiest CTA.
+// A walk list: n at [0], then the unit indices.
+__device__ __forceinline__ int list_count(const int *list) { return list[0]; }
 
 // Ring barriers come in plane pairs: planes 2p and 2p + 1 (sequence numbers)
 // share the "full" and "empty" mbarriers of pair slot p & (kPairs - 1), so a
@@ -890,16 +890,16 @@ __device__ __forceinline__ uint32_t empty_bar(const TSmem &S, uint32_t pair)
 // arrival there (a release), which the wait observes (an acquire) before the
 // asynchronous writes.  seq returns the number of planes issued; false if a
 // wait gave up (or another warp did).
-template <typename T, int G, int MODE>
-__device__ bool produce(const RJob *__restrict__ jobs, int64_t total, const Plan *__restrict__ plans,
+template <typename T, int G>
+__device__ bool produce(const RJob *__restrict__ jobs, const int *__restrict__ list, const Plan *__restrict__ plans,
                         const TSmem &S, uint32_t &seq)
 {
     using Gm = TGeom<T, G>;
     seq = 0;
     int last_job = -1;
-    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
-        const Plan P = plans[u];
-        if (!staged_in_mode<MODE>(P)) continue;
+    const int n = list_count(list);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const Plan P = plans[list[1 + i]];
         const RJob &J = jobs[P.j];
         if (P.j != last_job) {  // the descriptor was written by a copy
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&J.tmap) : "memory");
@@ -1596,12 +1596,55 @@ __global__ void __launch_bounds__(256) k_tps_plan(const RJob *__restrict__ jobs,
     }
 }
 
+// The staged walks as two lists in unit order (one CTA of 32 warps): l0 the
+// interior walks, l1 the others; each list's count at [0], the unit indices
+// after it.  Warp w compacts a contiguous range of units with ballots; the
+// ranges' offsets come from the warps' counts.
+__global__ void __launch_bounds__(1024) k_tps_lists(const Plan *__restrict__ plans, int64_t total, int *l0, int *l1)
+{
+    __shared__ int wc[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t per = (((total + 31) / 32) + 31) / 32 * 32;  // units per warp, a multiple of 32
+    const int64_t b = (int64_t)warp * per, e = min(total, b + per);
+    int c0 = 0, c1 = 0;
+    for (int64_t u0 = b; u0 < e; u0 += 32) {
+        const int64_t u = u0 + lane;
+        const bool st = u < e && plans[u].staged, in = st && plans[u].interior;
+        c0 += __popc(__ballot_sync(0xffffffffu, st && in));
+        c1 += __popc(__ballot_sync(0xffffffffu, st && !in));
+    }
+    if (lane == 0) {
+        wc[0][warp] = c0;
+        wc[1][warp] = c1;
+    }
+    __syncthreads();
+    int o0 = 0, o1 = 0;
+    for (int i = 0; i < warp; ++i) {
+        o0 += wc[0][i];
+        o1 += wc[1][i];
+    }
+    const unsigned below = (1u << lane) - 1u;
+    for (int64_t u0 = b; u0 < e; u0 += 32) {
+        const int64_t u = u0 + lane;
+        const bool st = u < e && plans[u].staged, in = st && plans[u].interior;
+        const unsigned m0 = __ballot_sync(0xffffffffu, st && in), m1 = __ballot_sync(0xffffffffu, st && !in);
+        if (st && in) l0[1 + o0 + __popc(m0 & below)] = (int)u;
+        if (st && !in) l1[1 + o1 + __popc(m1 & below)] = (int)u;
+        o0 += __popc(m0);
+        o1 += __popc(m1);
+    }
+    if (warp == 31 && lane == 0) {  // the last warp's end offsets are the totals
+        l0[0] = o0;
+        l1[0] = o1;
+    }
+}
+
 // TPS units whose source footprint is staged by TMA (trilinear), with the
 // plans of k_tps_plan; units without a staged plan are left to k_tps_gather.
 template <typename T, int G, int MODE>
-__global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__restrict__ jobs, int njobs,
-                                                                   int64_t total_units, const Plan *__restrict__ plans,
-                                                                   int *err)
+__global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__restrict__ jobs,
+                                                                   const int *__restrict__ list,
+                                                                   const Plan *__restrict__ plans, int *err)
 {
     using Gm = TGeom<T, G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1638,7 +1681,7 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
     if (warp == kRowWarps) {  // the producer warp: lane 0 issues every copy
         if (lane == 0) {
             uint32_t seq = 0;
-            if (!produce<T, G, MODE>(jobs, total_units, plans, S, seq)) {
+            if (!produce<T, G>(jobs, list, plans, S, seq)) {
                 *reinterpret_cast<volatile int *>(&abort_sh) = 1;  // the row warps see it in their waits
                 if (err) atomicOr(err, kKernErrTimeout);
             }
@@ -1650,9 +1693,9 @@ __global__ void __launch_bounds__(kStagedThreads, 1) k_tps_staged(const RJob *__
     const int x = 2 * lane;
     const float4 wx[2] = {S.W[x % G], S.W[(x + 1) % G]};
     RingPos R = {0u, 0u};
-    for (int64_t u = blockIdx.x; u < total_units; u += gridDim.x) {
-        const Plan P = plans[u];
-        if (!staged_in_mode<MODE>(P)) continue;  // the other launch, or the gather kernel, takes it
+    const int n = list_count(list);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const Plan P = plans[list[1 + i]];
         Walk w;
         w.j = P.j;
         w.Ox = P.ox;
@@ -1724,7 +1767,15 @@ cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_
         k_tps_plan<T, G><<<(unsigned)pgrid, 256, 0, st>>>(jobs, njobs, total, plans, fb);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        for (auto k : {k_tps_staged<T, G, 0>, k_tps_staged<T, G, 1>}) {  // interior walks, then the others
+        // the two walk lists after the plans: [count, units...] each
+        int *l0 = reinterpret_cast<int *>(plans + total);
+        int *l1 = l0 + 1 + total;
+        k_tps_lists<<<1, 1024, 0, st>>>(plans, total, l0, l1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const auto k0 = k_tps_staged<T, G, 0>, k1 = k_tps_staged<T, G, 1>;
+        for (int mode = 0; mode < 2; ++mode) {  // interior walks, then the others
+            const auto k = mode == 0 ? k0 : k1;
             e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Gm::smem_bytes);
             if (e != cudaSuccess) return e;
             int per_sm = 0;
@@ -1734,7 +1785,7 @@ cudaError_t launch_tps_t(const RJob *jobs, int njobs, int64_t total, cudaStream_
             int64_t grid = (int64_t)sms * per_sm;
             if (grid > total) grid = total;
             if (grid < 1) grid = 1;
-            k<<<(unsigned)grid, kStagedThreads, Gm::smem_bytes, st>>>(jobs, njobs, total, plans, err);
+            k<<<(unsigned)grid, kStagedThreads, Gm::smem_bytes, st>>>(jobs, mode == 0 ? l0 : l1, plans, err);
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
@@ -1785,7 +1836,9 @@ cudaError_t dispatch_g(const RJob *jobs, int njobs, int64_t total, int g, cudaSt
 
 size_t tps_stage_ws_bytes(int64_t total_bricks)
 {
-    return sizeof(int64_t) * (size_t)((1 + total_bricks + 1) & ~(int64_t)1) + sizeof(Plan) * (size_t)total_bricks;
+    // fallback list, plans, the two staged-walk lists
+    return sizeof(int64_t) * (size_t)((1 + total_bricks + 1) & ~(int64_t)1) + sizeof(Plan) * (size_t)total_bricks +
+           sizeof(int) * (size_t)(2 * (1 + total_bricks));
 }
 
 bool g_supported(int g) { return g == 4 || g == 8 || g == 16 || g == 32 || g == 64; }
