@@ -788,6 +788,13 @@ def run_ours(args):
                        "ms_per_step": e2e_s * 1e3}
         equal = bool(torch.equal(h_dst, dst.cpu()))
         line["e2e"]["matches_device_path"] = equal
+        # the host link bounds e2e: its bytes per step over the measured
+        # rate of pinned copies in both directions at once on this box
+        link = copy_peaks(local)
+        link_gbs = 2 * vox * 2 / e2e_s / 1e9
+        line["e2e"]["link"] = {"achieved_gbs": link_gbs, "both_directions_peak_gbs": link["both_gbs"],
+                               "frac": link_gbs / link["both_gbs"], "h2d_peak_gbs": link["h2d_gbs"],
+                               "d2h_peak_gbs": link["d2h_gbs"]}
         del h_src, h_dst
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy_leg(ctx, case, dst)
