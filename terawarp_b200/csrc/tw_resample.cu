@@ -966,6 +966,18 @@ __device__ __forceinline__ void release_plane(const TSmem &S, RingPos &R)
     ++R.rseq;
 }
 
+// Releases the two oldest planes the warp holds, s and s + 1, without a
+// test of their parity: whichever of them is the second plane of its pair
+// completes pair s / 2 (planes s, s + 1 when s is even; s - 1, released
+// before, and s when s is odd), and every lane arrives on that pair's
+// "empty" barrier.  A pair is completed by exactly one release, single or
+// double, so each lane arrives once per pair.
+__device__ __forceinline__ void release_two_planes(const TSmem &S, RingPos &R)
+{
+    mbar_arrive(empty_bar(S, R.rseq >> 1));
+    R.rseq += 2;
+}
+
 // The row warps' state of one cell layer (uniform across the warp except
 // the position pairs).
 struct RowLayer {
@@ -1373,8 +1385,8 @@ __device__ bool walk_rows(const RJob &J, const Walk &w, const Plan &P, const TSm
         prep(zoff, q, keep);
         // sequence past the last plane output plane Oz + pz reads
         uint32_t need = seq0 + (uint32_t)(zf - w.z0) + Wn;
-        for (int pz = zoff; pz < zend; ++pz, ++need) {
-            if (!wait_planes(S, R, need)) return false;
+        // one output plane, its planes already waited for
+        auto plane = [&](int pz) {
             float2 lo[NR][4], hi[NR][4];
 #pragma unroll
             for (int k = 0; k < NR; ++k) taps_pair<T>(q[k], lo[k], hi[k]);
@@ -1394,6 +1406,23 @@ __device__ bool walk_rows(const RJob &J, const Walk &w, const Plan &P, const TSm
                 if (BORDER) keep[k] = nkeep[k];
             }
             dp += dpz;
+        };
+        // interior walks take two output planes a step: one wait (the second
+        // plane's window reaches one plane further) and one release of both
+        // planes' oldest planes (border walks, one plane a step, keep their
+        // masks in registers that way)
+        int pz = zoff;
+        if constexpr (!BORDER) {
+            for (; pz + 1 < zend; pz += 2, need += 2) {
+                if (!wait_planes(S, R, need + 1)) return false;
+                plane(pz);
+                plane(pz + 1);
+                release_two_planes(S, R);
+            }
+        }
+        for (; pz < zend; ++pz, ++need) {
+            if (!wait_planes(S, R, need)) return false;
+            plane(pz);
             release_plane(S, R);
         }
         zf = ze;
