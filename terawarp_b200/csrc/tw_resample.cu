@@ -1093,15 +1093,19 @@ __device__ __forceinline__ void plane_positions(const RowLayer &L, float4 wz, fl
 }
 
 // Offset (from the ring base) of the (x, y, z) = floor tap of a staged
-// sample, from the magic-floor bit patterns; cz maps a tap plane to its
-// plane sequence (mod kRing: the slot); clamped so that all 8 taps stay in
-// the ring.
+// sample: the in-plane byte offset comes as the magic float kMagic + offset
+// (exact for offsets below 2^22 in magnitude, and every tap of the staged
+// window is), the slot from the z floor's magic bit pattern; cz maps a tap
+// plane to its plane sequence (mod kRing: the slot).  Clamped so that all 8
+// taps stay in the ring whatever the position (an out-of-range or NaN
+// position gives some offset in the ring, for a sample whose value the
+// range rule discards).
 template <typename T>
-__device__ __forceinline__ uint32_t staged_off(uint32_t kxy, uint32_t omax, uint32_t cz, float mx, float my, float mz)
+__device__ __forceinline__ uint32_t staged_off(uint32_t omax, uint32_t cz, float mz, float mxy)
 {
-    constexpr uint32_t ROW_B = kBoxW * sizeof(T), PLANE_B = kHMax * ROW_B;
+    constexpr uint32_t PLANE_B = kHMax * kBoxW * sizeof(T);
     const uint32_t slot = (__float_as_uint(mz) + cz) & (uint32_t)(kRing - 1);
-    const uint32_t o = slot * PLANE_B + __float_as_uint(my) * ROW_B + __float_as_uint(mx) * (uint32_t)sizeof(T) + kxy;
+    const uint32_t o = slot * PLANE_B + (__float_as_uint(mxy) - (uint32_t)kMagicBits);
     return min(o, omax);
 }
 
@@ -1127,19 +1131,25 @@ struct PairPrep {
     uint32_t a0, a1;  // shared-window addresses of the floor taps of voxel 0 / 1 in the ring
 };
 
-// ring: shared-window address of slot 0.
+// ring: shared-window address of slot 0; kc = kMagic + the byte offset of
+// frame (0, 0) in a plane slot.  The floors are integers below 2^22 in
+// magnitude, so fly ROW_B + flx ES + kc is exact whenever the tap lies in
+// the staged window.
 template <typename T>
-__device__ __forceinline__ PairPrep prep_pair(uint32_t ring, uint32_t kxy, uint32_t omax, uint32_t cz, float2 px,
+__device__ __forceinline__ PairPrep prep_pair(uint32_t ring, float kc, uint32_t omax, uint32_t cz, float2 px,
                                               float2 py, float2 pz)
 {
+    constexpr float ROW_B = (float)(kBoxW * sizeof(T)), ES = (float)sizeof(T);
     const float2 MM = f2(kMagic, kMagic);
     const float2 mx = __fadd2_rd(px, MM), my = __fadd2_rd(py, MM), mz = __fadd2_rd(pz, MM);
+    const float2 flx = sub2(mx, MM), fly = sub2(my, MM);
     PairPrep q;
-    q.fx = sub2(px, sub2(mx, MM));
-    q.fy = sub2(py, sub2(my, MM));
+    q.fx = sub2(px, flx);
+    q.fy = sub2(py, fly);
     q.fz = sub2(pz, sub2(mz, MM));
-    q.a0 = ring + staged_off<T>(kxy, omax, cz, mx.x, my.x, mz.x);
-    q.a1 = ring + staged_off<T>(kxy, omax, cz, mx.y, my.y, mz.y);
+    const float2 mxy = fma2(fly, f2(ROW_B, ROW_B), fma2(flx, f2(ES, ES), f2(kc, kc)));
+    q.a0 = ring + staged_off<T>(omax, cz, mz.x, mxy.x);
+    q.a1 = ring + staged_off<T>(omax, cz, mz.y, mxy.y);
     return q;
 }
 
@@ -1343,10 +1353,9 @@ __device__ bool walk_rows(const RJob &J, const Walk &w, const Plan &P, const TSm
     const int xe = BORDER ? (int)min(J.out_o[0] + J.out_n[0] - w.Ox, (int64_t)kTBX) : kTBX;
     const bool pair_ok =
         !BORDER || ((((uintptr_t)J.dst) % (2 * sizeof(T))) == 0 && (J.dst_py % 2 == 0) && (J.dst_pz % 2 == 0));
-    // frame (0, 0) in slot 0 minus the magic-float bias of the floor bit
-    // patterns (2^32 wrap arithmetic)
-    const uint32_t kxy =
-        (uint32_t)(P.DY - kMagicBits) * (uint32_t)Gm::ROW_B + (uint32_t)(P.DX - kMagicBits) * (uint32_t)Gm::ES;
+    // kMagic + the byte offset of frame (0, 0) in a plane slot (an integer
+    // below 2^14: exact)
+    const float kc = kMagic + (float)(P.DY * Gm::ROW_B + P.DX * Gm::ES);
     const uint32_t omax = (uint32_t)(kRing * Gm::PLANE_B - Gm::ROW_B - 2 * Gm::ES);
     for (int64_t zf = w.z0; zf < w.z1;) {
         const int64_t ze = min(w.z1, (zf / G + 1) * G);
@@ -1370,7 +1379,7 @@ __device__ bool walk_rows(const RJob &J, const Walk &w, const Plan &P, const TSm
             for (int k = 0; k < NR; ++k) {
                 float2 px, py, pz;
                 pair_positions(wz, PX[k], PY[k], PZ[k], px, py, pz);
-                q[k] = prep_pair<T>(S.sring, kxy, omax, cz, px, py, pz);
+                q[k] = prep_pair<T>(S.sring, kc, omax, cz, px, py, pz);
                 if (BORDER) {
                     const bool ok0 = px.x >= fr.lo[0] && px.x <= fr.hi[0] && py.x >= fr.lo[1] && py.x <= fr.hi[1] &&
                                      pz.x >= fr.lo[2] && pz.x <= fr.hi[2];
