@@ -755,7 +755,7 @@ def run_ours(args):
                    "volume_xyz": [X, Y, Z], "landmarks": n, "grid_spacing": G, "interp": "trilinear",
                    "parallelism": f"replicas x{ws}", "l2": "input 8 GiB > 126 MB L2 (no flush needed)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "kernel": ("k_tps_plan + k_tps_staged + k_tps_gather<uint16,16>" if args.resample == "staged"
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": ("k_tps_plan + k_tps_lists + k_tps_staged x2 + k_tps_gather<uint16,16>" if args.resample == "staged"
                                 else "k_tps_gather<uint16,16>"),
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": warp_avg},
         "gpu_launches": launches,
